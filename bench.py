@@ -1,0 +1,331 @@
+#!/usr/bin/env python3
+"""Benchmark: Bellman cell-control updates per second of the plain FP32
+value-iteration sweep on one B200 per rank.
+
+A step is one Jacobi sweep over the whole table (every cell x every control).
+Workload: 48 x 48 x 32 x 15 x 15 x 15 = 248,832,000 cells, 125 controls
+({-1,-0.5,0,0.5,1}^3), dt 0.04 s, RK2, 6 rectangular obstacles, seed 0 --
+one table per GPU; with --gpus N every rank solves its own independent table
+(different seed), so per-GPU work is fixed (weak scaling, no data-path
+collective; the only collective is the max of the timings).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference's CPU algorithm (the oracle port of
+solve.jl's sweep, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "peregrine-desktop_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Bellman cell-control updates/s; time-to-converge vs plain FP32 at ≤2 ms max err"
+UNIT = "cell-control updates/s"
+WORKLOAD = "medium"
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_stencil_medium_fp32.md")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the stencil kernel from the committed ncu
+    summary (a line `traffic_bytes_per_launch: N`), or None."""
+    if not os.path.exists(PROFILE_TRAFFIC):
+        return None
+    for line in open(PROFILE_TRAFFIC):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.fh = None
+
+    def __enter__(self):
+        try:
+            self.fh = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.fh is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.fh.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.fh.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(pr, budget_s: float, threads: int, rank_seed: int = 0):
+    """The oracle (a CPU restatement of the reference's sweep) on a bounded,
+    contiguous slab of cells in the middle of the table."""
+    import numpy as np
+    from oracle import oracle as og
+    g = og.copy_struct(pr.grid.to_c(), og.OGrid)
+    m = og.copy_struct(pr.model.to_c(), og.OModel)
+    p = og.copy_struct(pr.params, og.OParams)
+    V = np.full(pr.ncells, np.float32(pr.params.cap), np.float32)
+    V[pr.seeds] = 0.0
+    mid = pr.ncells // 2
+    probe = 8192 * max(1, threads)
+    t0 = time.perf_counter()
+    og.sweep_jacobi(V, pr.occ, g, m, pr.ctl, p, 0, mid, mid + probe, threads)
+    rate = probe / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(max(rate * budget_s, probe), pr.ncells // 4))
+    t0 = time.perf_counter()
+    og.sweep_jacobi(V, pr.occ, g, m, pr.ctl, p, 0, mid, mid + n, threads)
+    dt = time.perf_counter() - t0
+    return n, dt, n * pr.nctl / dt
+
+
+def problem_for_rank(rank: int):
+    from peregrine_hjb.synth import Problem
+    return Problem(WORKLOAD, seed=rank)
+
+
+def workload_config(pr, extra=None):
+    n = pr.grid.n
+    cfg = {
+        "workload": f"plain FP32 value iteration, {n[0]}x{n[1]}x{n[2]}x{n[3]}x{n[4]}x{n[5]} "
+                    f"= {pr.ncells} cells, {pr.nctl} controls (cube5), dt {pr.cfg['dt']} s, RK2, "
+                    f"6 rectangles, 64-corner multilinear, one table per GPU",
+        "cells": pr.ncells,
+        "controls": pr.nctl,
+        "step": "one Jacobi sweep over every cell and control",
+        "l2": "inputs larger than L2 (V is 0.995 GB per buffer, two buffers)",
+        "kernel": "k_stencil<float,float,FMA>",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the oracle port on all host threads, rank 0 only."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as og
+    threads = og.available_threads()
+    pr = problem_for_rank(0)
+    per_step = []
+    samples = []
+    for s in range(args.warmup + args.steps):
+        n, dt, rate = cpu_sample(pr, 6.0, threads)
+        if s >= args.warmup:
+            per_step.append(rate)
+            samples.append((n, dt))
+    value = statistics.mean(per_step)
+    n0 = samples[0][0]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * statistics.mean(dt for _, dt in samples),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded PCG64 job in the reference's input schemas)",
+        "impl": "reference",
+        "config": workload_config(pr, {"kernel": "CPU restatement of the reference sweep "
+                                                 "(oracle/pg_oracle.c), OpenMP"}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n0} contiguous cells x {pr.nctl} controls per step "
+                                   f"(one Jacobi pass over a mid-table slab, about 6 s)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from peregrine_hjb import _lib
+
+    torch.cuda.set_device(local_rank)
+    pr = problem_for_rank(rank)
+    ctx = _lib.Context(local_rank)
+    ctx.load_problem(pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.ctl, "fp32")
+    opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL)
+    # seed and take the warm-up sweeps (real Bellman updates from the seeded table)
+    ctx.solve(pr.seeds, max(args.warmup, 3), 0.0, opts)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident throughput: K sweeps, CUDA events on the launch stream
+    launches0 = ctx.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        ms = ctx.time_sweeps(0, args.steps, _lib.KERNEL_STENCIL)
+    torch.cuda.synchronize()
+    barrier()
+    launches = ctx.launch_count() - launches0
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cc_per_sweep = pr.ncells * pr.nctl
+    value = world * cc_per_sweep / (ms_max / 1000.0)
+
+    # ---- end to end through the public one-shot call, host buffers in/out
+    e2e_sweeps = 2
+    occ_h = torch.from_numpy(pr.occ).pin_memory()
+    ctl_h = torch.from_numpy(pr.ctl).pin_memory()
+    tidx_h = torch.from_numpy(pr.seeds).pin_memory()
+    V_h = torch.empty(pr.ncells, dtype=torch.float32).pin_memory()
+    occ_n, ctl_n, tidx_n, V_n = (x.numpy() for x in (occ_h, ctl_h, tidx_h, V_h))
+    e2e_steps = max(1, min(args.steps, 3))
+    import ctypes as C
+    lib = _lib.load_library()
+    res = _lib.SolveResult()
+    e2e_opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL)
+    cb = _lib.PROGRESS_CB()
+    times = []
+    for _ in range(e2e_steps + 1):
+        barrier()
+        t0 = time.perf_counter()
+        rc = lib.pg_solve_value(ctx._h, C.byref(pr.grid.to_c()), C.byref(pr.model.to_c()),
+                                C.byref(pr.params), occ_n.ctypes.data, tidx_n.ctypes.data,
+                                tidx_n.size, ctl_n.ctypes.data, pr.nctl, e2e_sweeps, 0.0,
+                                C.byref(e2e_opts), V_n.ctypes.data, C.byref(res), cb, None)
+        if rc != 0:
+            raise RuntimeError(lib.pg_last_error().decode())
+        times.append(time.perf_counter() - t0)
+    e2e_t = torch.tensor([statistics.mean(times[1:])], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_s = float(e2e_t.item())
+    e2e_value = world * e2e_sweeps * cc_per_sweep / e2e_s
+    h2d = pr.occ.nbytes + pr.ctl.nbytes + pr.seeds.nbytes
+    d2h = pr.ncells * 4
+    if not np.all(np.isfinite(V_n)):
+        raise RuntimeError("non-finite values in the solved table")
+
+    if rank != 0:
+        ctx.close()
+        return 0
+
+    # ---- roofline of the dominant kernel (the stencil sweep)
+    peak, peak_kind = peaks()
+    alg_bytes = 2 * 4 * pr.ncells  # read V once + write V once per sweep
+    achieved = alg_bytes / (ms / 1000.0) / 1e9
+    traffic = profiled_traffic()
+
+    # ---- CPU baseline: the oracle on the host cores, bounded sample
+    from oracle import oracle as og
+    threads = og.available_threads()
+    n_cpu, dt_cpu, cpu_rate = cpu_sample(pr, 12.0, threads)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded PCG64 job in the reference's input schemas)",
+        "config": workload_config(pr, {"parallelism": f"{world} independent tables, one per GPU"}),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n_cpu} contiguous cells x {pr.nctl} controls, one Jacobi "
+                                   f"pass ({dt_cpu:.1f} s) of the same workload"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "step": f"one pg_solve_value call: upload occupancy/controls/seeds, "
+                        f"{e2e_sweeps} sweeps, read V back to pinned host memory"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

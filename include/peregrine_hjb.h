@@ -1,0 +1,218 @@
+/*
+ * peregrine_hjb.h -- C ABI of libperegrine_hjb.so, the B200 (sm_100a)
+ * minimum-time value-table solver.
+ *
+ * This library replaces the value-iteration solve that Peregrine-Desktop's
+ * `solver/solve.jl` drives through `solve_value!` (solver/src/Run.jl:1434-1474)
+ * and the CUDA.jl sweep kernels behind it (solver/src/Gpu.jl:5-37). It is a
+ * plain C interface: POD structs, pointers and sizes, no C++ or torch types.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: PG_OK (0) or a negative PG_E*
+ *     code.  The message of the last failure on the calling thread is
+ *     available from pg_last_error().  No exception ever crosses the ABI.
+ *   - Flat cell indices are 0-based and follow the table's row-major order
+ *     ((((ix*Ny+iy)*Nh+ih)*Nvx+ivx)*Nvy+ivy)*Nw+iw (docs/TABLE_FORMAT.md §4).
+ *     The reference passes 1-based indices (`seeds = tcells .+ 1`,
+ *     Run.jl:1853); this ABI does not add the 1.
+ *   - The caller owns every host buffer; a context owns its device buffers.
+ *     One context per host thread; each context has its own CUDA stream.
+ *   - Progress callbacks run on the calling thread, between sweeps.
+ */
+#ifndef PEREGRINE_HJB_H
+#define PEREGRINE_HJB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PG_ABI_VERSION 1
+
+/* status codes */
+#define PG_OK            0
+#define PG_EINVAL       -1   /* bad argument (the reference's `error(...)`)   */
+#define PG_ECUDA        -2   /* a CUDA runtime call failed                     */
+#define PG_ENOMEM       -3   /* device allocation failed or would not fit      */
+#define PG_ETIMEOUT     -4   /* a bounded device wait gave up                  */
+#define PG_ESTATE       -5   /* call out of order (no problem loaded, ...)     */
+#define PG_EUNSUPPORTED -6   /* option combination not implemented             */
+#define PG_ECANCELLED   -7   /* the progress callback asked to stop            */
+
+/* Grid6 (solver/src/PeregrineSolver.jl:47-51): samples per axis, axis origin
+ * and step.  Axis 2 (heading) is periodic with lo = -pi, step = 2pi/n. */
+typedef struct pg_grid6 {
+    int32_t n[6];
+    float lo[6];
+    float step[6];
+} pg_grid6;
+
+/* Model (PeregrineSolver.jl:100-109): row-major 3x3 blocks. */
+typedef struct pg_model {
+    float B[9];     /* control                          */
+    float A[9];     /* velocity                         */
+    float q[3];     /* omega^2                          */
+    float S[9];     /* Coulomb, multiplies csign(v)     */
+    float D[9];     /* quadratic drag, multiplies |v|v  */
+    float c[3];     /* constant                         */
+    float eps[3];   /* Coulomb smoothing band           */
+    float knee;     /* traction knee; <= 0 or NaN disables saturation */
+} pg_model;
+
+/* Params (PeregrineSolver.jl:897-916).  Booleans are int32 0/1. */
+typedef struct pg_params {
+    float dt;
+    int32_t nsub;
+    int32_t checks;
+    int32_t adaptive_checks;
+    int32_t nearest;
+    float cap;
+    int32_t ntau;
+    float tau_ratio;
+    float cfl;
+    float tau_min;
+    float tau_max;
+    float hmax;
+    int32_t ncoarse;
+    int32_t rounds;
+    float delta0;
+    int32_t rk2;
+    int32_t vclamp;
+    int32_t simplex;
+} pg_params;
+
+/* Stop rule.  L1_QUIET is the reference's: total improvement of a sweep
+ * <= tol for ceil((nctl-1)/ncoarse) consecutive sweeps (Run.jl:1441-1471).
+ * MAXNORM stops on the largest single-cell change instead. */
+#define PG_STOP_L1_QUIET 0
+#define PG_STOP_MAXNORM  1
+
+/* Storage of V on the device.  Arithmetic is FP32 for F32/F16/BF16 and FP64
+ * for F64 (the FP64 device oracle). */
+#define PG_STORE_F32  0
+#define PG_STORE_F16  1
+#define PG_STORE_BF16 2
+#define PG_STORE_F64  3
+
+/* Sweep kernel selection. */
+#define PG_KERNEL_AUTO     0  /* stencil when the scheme allows it, else cellform */
+#define PG_KERNEL_STENCIL  1  /* position-invariant stencil (plain scheme)     */
+#define PG_KERNEL_CELLFORM 2  /* one thread per cell, the full cell_update     */
+#define PG_KERNEL_STENCIL_EXACT 3 /* stencil with the reference's rounding order */
+
+/* Table dtypes (solver/src/Pipeline.jl:620-625). */
+#define PG_DTYPE_U8  0
+#define PG_DTYPE_U16 1
+#define PG_DTYPE_F16 2
+#define PG_DTYPE_F32 3
+
+typedef struct pg_solve_opts {
+    int32_t stop_rule;      /* PG_STOP_*                                         */
+    int32_t storage;        /* PG_STORE_*                                        */
+    int32_t kernel;         /* PG_KERNEL_*                                       */
+    int32_t warm_start;     /* keep the Int8 warm-start policy (Run.jl:1784)     */
+    int32_t polish_sweeps;  /* 16-bit storage: max FP32 sweeps after convergence */
+    int32_t progress_every; /* callback cadence; 0 = reference cadence (it%5, 1, last) */
+    int32_t reserved[6];
+} pg_solve_opts;
+
+typedef struct pg_solve_result {
+    int32_t iterations;     /* sweeps run (16-bit phase + polish)                */
+    int32_t polish_iterations;
+    double last_delta;      /* L1 total improvement of the last sweep            */
+    double last_maxnorm;    /* largest single-cell improvement of the last sweep */
+    double kernel_ms;       /* device time of the sweeps (CUDA events)           */
+    double elapsed_ms;      /* host wall time of the call                        */
+    int64_t cell_controls;  /* lookaheads evaluated over all sweeps (all cells)  */
+} pg_solve_result;
+
+/* Return nonzero to cancel the solve (PG_ECANCELLED). */
+typedef int (*pg_progress_cb)(void* user, int32_t iter, double delta, double maxnorm);
+
+typedef struct pg_ctx pg_ctx;
+
+/* ------------------------------------------------------------------ */
+/* library                                                             */
+/* ------------------------------------------------------------------ */
+int32_t pg_abi_version(void);
+const char* pg_last_error(void);
+void pg_default_opts(pg_solve_opts* opts);
+
+/* Create a context on CUDA device `device`; its own stream. */
+int pg_create(pg_ctx** out, int device);
+int pg_destroy(pg_ctx* ctx);
+
+/* ------------------------------------------------------------------ */
+/* one-shot solve: the drop-in for solve_value!                        */
+/*   solve_value!(V, occ, g, m, tidx, ctl, nctl, p; iters, tol, ...)   */
+/*   (solver/src/Run.jl:1434-1474)                                     */
+/* occ: Nx*Ny*Nh bytes, index (ix*Ny+iy)*Nh+ih (Pipeline.jl:393-398).  */
+/* ctl: planar [u1(nctl) u2(nctl) u3(nctl)] (Run.jl:283-285).          */
+/* tidx: 0-based seeded target cells.  V_out: ncells floats, row-major */
+/* (may be NULL to keep V on the device for pg_get_value/pg_encode).   */
+/* ------------------------------------------------------------------ */
+int pg_solve_value(pg_ctx* ctx, const pg_grid6* g, const pg_model* m,
+                   const pg_params* p, const uint8_t* occ,
+                   const int64_t* tidx, int64_t ntidx,
+                   const float* ctl, int32_t nctl,
+                   int32_t iters, double tol, const pg_solve_opts* opts,
+                   float* V_out, pg_solve_result* res,
+                   pg_progress_cb cb, void* user);
+
+/* ------------------------------------------------------------------ */
+/* staged use: load the problem once, then solve / sweep / read        */
+/* ------------------------------------------------------------------ */
+
+/* Upload grid, model, params, occupancy and control table and allocate the
+ * device value buffers for `storage`.  Replaces the allocations of
+ * run_solve (Run.jl:1776-1784). */
+int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m,
+                    const pg_params* p, const uint8_t* occ,
+                    const float* ctl, int32_t nctl, int32_t storage);
+
+/* Seed and iterate on the loaded problem (solve_value!, Run.jl:1434-1474). */
+int pg_solve(pg_ctx* ctx, const int64_t* tidx, int64_t ntidx, int32_t iters,
+             double tol, const pg_solve_opts* opts, pg_solve_result* res,
+             pg_progress_cb cb, void* user);
+
+/* Device V <-> host, row-major f32 (the reference's Array(V), Run.jl:1954). */
+int pg_get_value(pg_ctx* ctx, float* V_out);
+int pg_set_value(pg_ctx* ctx, const float* V_in);
+
+/* One Jacobi sweep V <- min(V, T V) on the loaded problem, `phase` as in
+ * sweep_gpu! (Gpu.jl:27-37).  delta = L1 total improvement, maxnorm = the
+ * largest single-cell improvement.  When `argmin_out` is non-NULL it gets,
+ * per cell (row-major), the index of the winning control in the control
+ * table, or -1 for a blocked cell. */
+int pg_sweep(pg_ctx* ctx, int32_t phase, int32_t kernel, double* delta,
+             double* maxnorm, int16_t* argmin_out);
+
+/* One escape sweep (Gpu.jl:51-80 semantics, Jacobi) on the loaded V. */
+int pg_escape_sweep(pg_ctx* ctx, int32_t phase, double* delta);
+
+/* Escape pass driver (solve_escape!, Run.jl:1503-1530). */
+int pg_solve_escape(pg_ctx* ctx, int32_t iters, double tol,
+                    pg_solve_result* res, pg_progress_cb cb, void* user);
+
+/* Encode V[lo, lo+n) (row-major) on the device into a host buffer
+ * (encode_into!, Pipeline.jl:698-780).  out must hold n*elem_bytes. */
+int pg_encode(pg_ctx* ctx, int32_t dtype, double scale, double escape_scale,
+              int64_t lo, int64_t n, uint8_t* out, int64_t* reached,
+              int64_t* escaped);
+
+/* Device-timed sweeps on the loaded, seeded problem: runs `warmup` untimed
+ * and `steps` timed sweeps with CUDA events on the context stream and
+ * returns the mean milliseconds per sweep.  No host copies inside. */
+int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
+                   double* ms_per_sweep);
+
+/* Number of this library's kernel launches since the context was created. */
+int pg_launch_count(pg_ctx* ctx, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PEREGRINE_HJB_H */

@@ -1,0 +1,662 @@
+// pg_api.cu -- the C ABI of libperegrine_hjb.so (include/peregrine_hjb.h).
+//
+// A context owns one CUDA stream and the device buffers of one loaded
+// problem: two value buffers (Jacobi ping-pong), the occupancy in (h, x, y)
+// order, the control table, the Int8 warm-start policy and the per-block
+// reduction partials.  The sweep loop of solve_value! (Run.jl:1434-1474) runs
+// here: one sweep kernel and one fixed-order reduction per sweep, a 16-byte
+// read of the two convergence numbers, the seed re-assertion, the stop rule.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pg_kernels.h"
+#include "pg_types.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define PG_CUDA(call)                                                                    \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(e_ == cudaErrorMemoryAllocation ? PG_ENOMEM : PG_ECUDA,          \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    } while (0)
+
+size_t elem_bytes(int storage) {
+    switch (storage) {
+        case PG_STORE_F32: return 4;
+        case PG_STORE_F16: return 2;
+        case PG_STORE_BF16: return 2;
+        case PG_STORE_F64: return 8;
+    }
+    return 0;
+}
+
+// substeps_for on the host, same float arithmetic as the device
+// (PeregrineSolver.jl:985-989).
+int32_t host_substeps_for(float tau, const pg_params& p) {
+    if (p.hmax <= 0.0f) return p.nsub;
+    volatile float q = tau / p.hmax;
+    float qq = q < 1.0e4f ? q : 1.0e4f;
+    int32_t k = (int32_t)qq + 1;
+    return k < 1 ? 1 : (k > 64 ? 64 : k);
+}
+
+}  // namespace
+
+struct pg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t launches = 0;
+
+    bool loaded = false;
+    pg::KParams kp{};
+    int base_storage = PG_STORE_F32;  // storage the problem was loaded with
+    int storage = PG_STORE_F32;       // storage of V right now (polish switches it)
+    bool stencil_ok = false;
+    std::string stencil_why;
+    std::vector<float> ctl_h;
+
+    void* V[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint8_t* occ_d = nullptr;
+    float* ctl_d = nullptr;
+    int8_t* pol_d = nullptr;
+    double* part_sum = nullptr;
+    double* part_max = nullptr;
+    int64_t nparts = 0;
+    double* red_d = nullptr;
+    double* red_h = nullptr;  // pinned [2]
+    int64_t* tidx_d = nullptr;
+    int64_t tidx_cap = 0;
+    int64_t ntidx = 0;
+    int16_t* argmin_d = nullptr;
+    uint8_t* enc_d = nullptr;
+    size_t enc_cap = 0;
+    unsigned long long* counts_d = nullptr;
+    float* stage_d = nullptr;  // row-major f32 staging for get/set
+    size_t stage_cap = 0;
+
+    void free_values() {
+        for (int i = 0; i < 2; ++i) {
+            if (V[i]) cudaFree(V[i]);
+            V[i] = nullptr;
+        }
+    }
+    void free_problem() {
+        free_values();
+        if (occ_d) cudaFree(occ_d);
+        if (ctl_d) cudaFree(ctl_d);
+        if (pol_d) cudaFree(pol_d);
+        if (part_sum) cudaFree(part_sum);
+        if (part_max) cudaFree(part_max);
+        if (tidx_d) cudaFree(tidx_d);
+        if (argmin_d) cudaFree(argmin_d);
+        if (enc_d) cudaFree(enc_d);
+        if (stage_d) cudaFree(stage_d);
+        occ_d = nullptr; ctl_d = nullptr; pol_d = nullptr; part_sum = nullptr;
+        part_max = nullptr; tidx_d = nullptr; argmin_d = nullptr; enc_d = nullptr;
+        stage_d = nullptr;
+        tidx_cap = 0; enc_cap = 0; stage_cap = 0; nparts = 0; ntidx = 0;
+        loaded = false;
+    }
+};
+
+namespace {
+
+int check_ctx(pg_ctx* ctx, bool need_problem) {
+    if (!ctx) return fail(PG_EINVAL, "null context");
+    if (need_problem && !ctx->loaded) return fail(PG_ESTATE, "no problem loaded");
+    if (cudaSetDevice(ctx->device) != cudaSuccess)
+        return fail(PG_ECUDA, "cudaSetDevice failed");
+    return PG_OK;
+}
+
+int ensure_stage(pg_ctx* ctx) {
+    size_t need = (size_t)ctx->kp.ncells * sizeof(float);
+    if (ctx->stage_cap >= need) return PG_OK;
+    if (ctx->stage_d) cudaFree(ctx->stage_d);
+    ctx->stage_d = nullptr;
+    ctx->stage_cap = 0;
+    PG_CUDA(cudaMalloc(&ctx->stage_d, need));
+    ctx->stage_cap = need;
+    return PG_OK;
+}
+
+// Make V buffers match `storage` (reallocating when the polish phase left
+// them in FP32).
+int ensure_values(pg_ctx* ctx, int storage) {
+    if (ctx->V[0] && ctx->storage == storage) return PG_OK;
+    ctx->free_values();
+    const size_t bytes = (size_t)ctx->kp.ncells * elem_bytes(storage);
+    size_t fr = 0, tot = 0;
+    PG_CUDA(cudaMemGetInfo(&fr, &tot));
+    if (2 * bytes > fr)
+        return fail(PG_ENOMEM, "the whole-grid solve needs " +
+                                   std::to_string(2.0 * bytes / (1 << 30)) +
+                                   " GiB of device memory for V but only " +
+                                   std::to_string((double)fr / (1 << 30)) + " GiB is free");
+    for (int i = 0; i < 2; ++i) PG_CUDA(cudaMalloc(&ctx->V[i], bytes));
+    ctx->storage = storage;
+    ctx->cur = 0;
+    return PG_OK;
+}
+
+int pick_kernel(pg_ctx* ctx, int32_t kernel, int* out) {
+    if (kernel == PG_KERNEL_AUTO) kernel = ctx->stencil_ok ? PG_KERNEL_STENCIL : PG_KERNEL_CELLFORM;
+    if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_EXACT) && !ctx->stencil_ok)
+        return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
+    if (kernel < PG_KERNEL_STENCIL || kernel > PG_KERNEL_STENCIL_EXACT)
+        return fail(PG_EINVAL, "unknown kernel " + std::to_string(kernel));
+    *out = kernel;
+    return PG_OK;
+}
+
+// One Jacobi sweep V[cur] -> V[1-cur]; does NOT read the residual back.
+int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmin_d,
+                bool use_pol) {
+    ctx->kp.phase = phase;
+    pg::SweepBufs sb{ctx->part_sum, ctx->part_max, ctx->nparts, ctx->red_d};
+    const void* vin = ctx->V[ctx->cur];
+    void* vout = ctx->V[1 - ctx->cur];
+    cudaError_t e;
+    if (esc || kernel == PG_KERNEL_CELLFORM)
+        e = pg::launch_cellform(ctx->storage, esc, vin, vout, ctx->occ_d,
+                                use_pol ? ctx->pol_d : nullptr, ctx->kp, ctx->ctl_d, sb, argmin_d,
+                                ctx->stream, &ctx->launches);
+    else
+        e = pg::launch_stencil(ctx->storage, kernel == PG_KERNEL_STENCIL_EXACT, vin, vout,
+                               ctx->occ_d, ctx->kp, ctx->ctl_d, sb, argmin_d, ctx->stream,
+                               &ctx->launches);
+    if (e != cudaSuccess) return fail(PG_ECUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
+    ctx->cur = 1 - ctx->cur;
+    return PG_OK;
+}
+
+int read_residual(pg_ctx* ctx, double* d, double* dm) {
+    PG_CUDA(cudaMemcpyAsync(ctx->red_h, ctx->red_d, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *d = ctx->red_h[0];
+    *dm = ctx->red_h[1];
+    return PG_OK;
+}
+
+int reseed(pg_ctx* ctx) {
+    if (ctx->ntidx <= 0) return PG_OK;
+    cudaError_t e = pg::launch_seed_only(ctx->storage, ctx->V[ctx->cur], ctx->kp, ctx->tidx_d,
+                                         ctx->ntidx, ctx->stream);
+    ctx->launches += 1;
+    if (e != cudaSuccess) return fail(PG_ECUDA, std::string("seed: ") + cudaGetErrorString(e));
+    return PG_OK;
+}
+
+// The iteration of solve_value! / solve_escape! (Run.jl:1441-1472, 1509-1528)
+int iterate(pg_ctx* ctx, int kernel, bool esc, int32_t iters, double tol, int stop_rule,
+            bool use_pol, int32_t progress_every, int32_t it0, pg_progress_cb cb, void* user,
+            int32_t* done_out, double* d_out, double* dm_out, double* kms, bool* converged) {
+    const pg_params& p = ctx->kp.p;
+    const int32_t nctl = ctx->kp.nctl;
+    int quiet_needed = 1;
+    if (p.ncoarse > 0) {
+        int q = (nctl - 1 + p.ncoarse - 1) / p.ncoarse;
+        quiet_needed = q > 1 ? q : 1;
+    }
+    double d = INFINITY, dm = INFINITY;
+    int quiet = 0;
+    int32_t done = 0;
+    *converged = false;
+    for (int32_t it = 1; it <= iters; ++it) {
+        PG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+        int rc = sweep_async(ctx, kernel, it0 + it - 1, esc, nullptr, use_pol);
+        if (rc) return rc;
+        PG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+        if (!esc) {
+            rc = reseed(ctx);
+            if (rc) return rc;
+        }
+        rc = read_residual(ctx, &d, &dm);
+        if (rc) return rc;
+        float ms = 0.0f;
+        PG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        *kms += ms;
+        done = it;
+        const double crit = stop_rule == PG_STOP_MAXNORM ? dm : d;
+        quiet = crit <= tol ? quiet + 1 : 0;
+        const bool stop = quiet >= quiet_needed;
+        const bool report = progress_every > 0 ? (it % progress_every == 0 || it == 1 || stop)
+                                               : (it % 5 == 0 || it == 1 || stop);
+        if (cb && report && cb(user, it0 + it, d, dm)) {
+            *done_out = done; *d_out = d; *dm_out = dm;
+            return fail(PG_ECANCELLED, "cancelled by the progress callback");
+        }
+        if (stop) { *converged = true; break; }
+    }
+    *done_out = done;
+    *d_out = d;
+    *dm_out = dm;
+    return PG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t pg_abi_version(void) { return PG_ABI_VERSION; }
+
+const char* pg_last_error(void) { return g_err.c_str(); }
+
+void pg_default_opts(pg_solve_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->stop_rule = PG_STOP_L1_QUIET;
+    o->storage = PG_STORE_F32;
+    o->kernel = PG_KERNEL_AUTO;
+    o->warm_start = 0;
+    o->polish_sweeps = 64;
+    o->progress_every = 0;
+}
+
+int pg_create(pg_ctx** out, int device) {
+    if (!out) return fail(PG_EINVAL, "null output pointer");
+    int n = 0;
+    PG_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n)
+        return fail(PG_EINVAL, "device " + std::to_string(device) + " out of range (" +
+                                   std::to_string(n) + " visible)");
+    PG_CUDA(cudaSetDevice(device));
+    pg_ctx* c = new pg_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaMalloc(&c->red_d, 2 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&c->red_h, 2 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->counts_d, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+        delete c;
+        return fail(PG_ECUDA, "context creation failed");
+    }
+    *out = c;
+    return PG_OK;
+}
+
+int pg_destroy(pg_ctx* ctx) {
+    if (!ctx) return PG_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->free_problem();
+    if (ctx->red_d) cudaFree(ctx->red_d);
+    if (ctx->red_h) cudaFreeHost(ctx->red_h);
+    if (ctx->counts_d) cudaFree(ctx->counts_d);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PG_OK;
+}
+
+int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                    const uint8_t* occ, const float* ctl, int32_t nctl, int32_t storage) {
+    int rc = check_ctx(ctx, false);
+    if (rc) return rc;
+    if (!g || !m || !p || !occ || !ctl) return fail(PG_EINVAL, "null argument");
+    for (int k = 0; k < 6; ++k)
+        if (g->n[k] < 2)
+            return fail(PG_EINVAL, "every axis needs at least 2 samples (Grid6)");
+    for (int k = 0; k < 6; ++k)
+        if (!(g->step[k] > 0.0f) || !std::isfinite(g->lo[k]))
+            return fail(PG_EINVAL, "grid steps must be positive and origins finite");
+    if (nctl < 2 || nctl > 32767)
+        return fail(PG_EINVAL, "the control table needs coast plus at least one command");
+    if (elem_bytes(storage) == 0) return fail(PG_EINVAL, "unknown storage");
+    if (!(p->cap > 0.0f)) return fail(PG_EINVAL, "value_cap must be positive");
+    if (p->nsub < 1) return fail(PG_EINVAL, "substeps must be >= 1");
+    if (p->checks < 1) return fail(PG_EINVAL, "sweep_checks must be >= 1");
+    if (!(p->dt > 0.0f)) return fail(PG_EINVAL, "dt must be positive");
+
+    ctx->free_problem();
+    pg::KParams& kp = ctx->kp;
+    std::memset(&kp, 0, sizeof(kp));
+    kp.g = *g;
+    kp.m = *m;
+    kp.p = *p;
+    kp.P = (int64_t)g->n[0] * g->n[1];
+    kp.nplanes = (int64_t)g->n[2] * g->n[3] * g->n[4] * g->n[5];
+    kp.ncells = kp.P * kp.nplanes;
+    kp.nctl = nctl;
+    // x rows per stencil block: about 2048 cells, never more than the plane
+    int32_t tx = (int32_t)((2048 + g->n[1] - 1) / g->n[1]);
+    if (tx < 1) tx = 1;
+    if (tx > g->n[0]) tx = g->n[0];
+    kp.tile_x = tx;
+    kp.tiles_x = (g->n[0] + tx - 1) / tx;
+    kp.nsub = host_substeps_for(p->cfl <= 0.0f ? p->dt : p->tau_max, *p);
+    kp.nchk = p->checks;
+
+    // Which schemes the position-invariant stencil reproduces exactly.
+    ctx->stencil_ok = true;
+    ctx->stencil_why.clear();
+    auto no = [&](const char* why) {
+        if (ctx->stencil_ok) ctx->stencil_why = why;
+        ctx->stencil_ok = false;
+    };
+    if (p->cfl > 0.0f) no("cfl > 0 (per-cell horizon)");
+    if (p->ntau > 1) no("tau_levels > 1 (horizon ladder)");
+    if (p->ncoarse > 0 && p->ncoarse < nctl - 1) no("control_scan rotates a partial slice");
+    if (p->rounds > 0) no("refine_rounds > 0 (pattern search)");
+    if (p->adaptive_checks) no("adaptive_checks");
+    if (p->nearest) no("nearest");
+    if (p->simplex) no("simplex (Kuhn) interpolation");
+    if (kp.nsub > pg::kStencilMaxSub) no("more than 16 substeps");
+    if (p->checks > pg::kStencilMaxChk) no("more than 24 probes");
+    if (kp.ncells / kp.tiles_x > (int64_t)1 << 40) no("grid too large");
+
+    ctx->ctl_h.assign(ctl, ctl + 3 * nctl);
+    ctx->base_storage = storage;
+    rc = ensure_values(ctx, storage);
+    if (rc) { ctx->free_problem(); return rc; }
+
+    const int32_t nx = g->n[0], ny = g->n[1], nh = g->n[2];
+    std::vector<uint8_t> occ_hxy((size_t)nx * ny * nh);
+    for (int32_t i = 0; i < nx; ++i)
+        for (int32_t j = 0; j < ny; ++j)
+            for (int32_t k = 0; k < nh; ++k)
+                occ_hxy[((size_t)k * nx + i) * ny + j] = occ[((size_t)i * ny + j) * nh + k] ? 1 : 0;
+    PG_CUDA(cudaMalloc(&ctx->occ_d, occ_hxy.size()));
+    PG_CUDA(cudaMemcpyAsync(ctx->occ_d, occ_hxy.data(), occ_hxy.size(), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    PG_CUDA(cudaMalloc(&ctx->ctl_d, sizeof(float) * 3 * nctl));
+    PG_CUDA(cudaMemcpyAsync(ctx->ctl_d, ctl, sizeof(float) * 3 * nctl, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    ctx->nparts = pg::cellform_blocks(kp.ncells);
+    const int64_t sb = pg::stencil_blocks(kp);
+    if (sb > ctx->nparts) ctx->nparts = sb;
+    PG_CUDA(cudaMalloc(&ctx->part_sum, sizeof(double) * ctx->nparts));
+    PG_CUDA(cudaMalloc(&ctx->part_max, sizeof(double) * ctx->nparts));
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->loaded = true;
+    return PG_OK;
+}
+
+int pg_solve(pg_ctx* ctx, const int64_t* tidx, int64_t ntidx, int32_t iters, double tol,
+             const pg_solve_opts* opts_in, pg_solve_result* res, pg_progress_cb cb, void* user) {
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    pg_solve_opts opts;
+    if (opts_in) opts = *opts_in;
+    else pg_default_opts(&opts);
+    if (ntidx < 0 || (ntidx > 0 && !tidx)) return fail(PG_EINVAL, "bad seed list");
+    if (iters < 0) return fail(PG_EINVAL, "iterations must be >= 0");
+    for (int64_t t = 0; t < ntidx; ++t)
+        if (tidx[t] < 0 || tidx[t] >= ctx->kp.ncells)
+            return fail(PG_EINVAL, "seed index " + std::to_string(tidx[t]) + " outside the grid");
+    int kernel = 0;
+    rc = pick_kernel(ctx, opts.warm_start && opts.kernel == PG_KERNEL_AUTO ? PG_KERNEL_CELLFORM
+                                                                          : opts.kernel,
+                     &kernel);
+    if (rc) return rc;
+    if (opts.warm_start && kernel != PG_KERNEL_CELLFORM)
+        return fail(PG_EUNSUPPORTED, "the warm-start policy needs the cell-form kernel");
+    rc = ensure_values(ctx, ctx->base_storage);
+    if (rc) return rc;
+
+    if (ntidx > ctx->tidx_cap) {
+        if (ctx->tidx_d) cudaFree(ctx->tidx_d);
+        ctx->tidx_d = nullptr;
+        PG_CUDA(cudaMalloc(&ctx->tidx_d, sizeof(int64_t) * ntidx));
+        ctx->tidx_cap = ntidx;
+    }
+    if (ntidx > 0)
+        PG_CUDA(cudaMemcpyAsync(ctx->tidx_d, tidx, sizeof(int64_t) * ntidx, cudaMemcpyHostToDevice,
+                                ctx->stream));
+    ctx->ntidx = ntidx;
+    if (opts.warm_start) {
+        if (!ctx->pol_d) PG_CUDA(cudaMalloc(&ctx->pol_d, (size_t)ctx->kp.ncells * 3));
+        PG_CUDA(cudaMemsetAsync(ctx->pol_d, 0, (size_t)ctx->kp.ncells * 3, ctx->stream));
+    }
+    ctx->cur = 0;
+    cudaError_t e = pg::launch_fill_seed(ctx->storage, ctx->V[0], ctx->kp, ctx->tidx_d, ntidx,
+                                         ctx->stream);
+    ctx->launches += ntidx > 0 ? 2 : 1;
+    if (e != cudaSuccess) return fail(PG_ECUDA, std::string("fill: ") + cudaGetErrorString(e));
+
+    int32_t done = 0, pdone = 0;
+    double d = INFINITY, dm = INFINITY, kms = 0.0;
+    bool conv = false;
+    rc = iterate(ctx, kernel, false, iters, tol, opts.stop_rule, opts.warm_start != 0,
+                 opts.progress_every, 0, cb, user, &done, &d, &dm, &kms, &conv);
+    if (rc) return rc;
+
+    // 16-bit storage: continue in FP32 from the converged 16-bit table until
+    // the same stop rule holds at FP32 resolution.
+    if ((ctx->storage == PG_STORE_F16 || ctx->storage == PG_STORE_BF16) && opts.polish_sweeps > 0) {
+        const size_t bytes = (size_t)ctx->kp.ncells * 4;
+        void* nv[2] = {nullptr, nullptr};
+        PG_CUDA(cudaMalloc(&nv[0], bytes));
+        if (cudaMalloc(&nv[1], bytes) != cudaSuccess) {
+            cudaFree(nv[0]);
+            return fail(PG_ENOMEM, "no room for the FP32 polish buffers");
+        }
+        e = pg::launch_convert_to_f32(ctx->storage, ctx->V[ctx->cur], (float*)nv[0],
+                                      ctx->kp.ncells, ctx->stream);
+        ctx->launches += 1;
+        if (e != cudaSuccess) { cudaFree(nv[0]); cudaFree(nv[1]); return fail(PG_ECUDA, "convert"); }
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->free_values();
+        ctx->V[0] = nv[0];
+        ctx->V[1] = nv[1];
+        ctx->cur = 0;
+        ctx->storage = PG_STORE_F32;
+        double d2 = d, dm2 = dm;
+        bool conv2 = false;
+        rc = iterate(ctx, kernel, false, opts.polish_sweeps, tol, opts.stop_rule,
+                     opts.warm_start != 0, opts.progress_every, done, cb, user, &pdone, &d2, &dm2,
+                     &kms, &conv2);
+        if (rc) return rc;
+        d = d2;
+        dm = dm2;
+    }
+    if (res) {
+        res->iterations = done + pdone;
+        res->polish_iterations = pdone;
+        res->last_delta = d;
+        res->last_maxnorm = dm;
+        res->kernel_ms = kms;
+        res->cell_controls = (int64_t)(done + pdone) * ctx->kp.ncells * ctx->kp.nctl;
+        res->elapsed_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return PG_OK;
+}
+
+int pg_get_value(pg_ctx* ctx, float* V_out) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (!V_out) return fail(PG_EINVAL, "null output");
+    rc = ensure_stage(ctx);
+    if (rc) return rc;
+    cudaError_t e = pg::launch_to_rowmajor(ctx->storage, ctx->V[ctx->cur], ctx->stage_d, ctx->kp,
+                                           ctx->stream);
+    ctx->launches += 1;
+    if (e != cudaSuccess) return fail(PG_ECUDA, "to_rowmajor");
+    PG_CUDA(cudaMemcpyAsync(V_out, ctx->stage_d, (size_t)ctx->kp.ncells * 4, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PG_OK;
+}
+
+int pg_set_value(pg_ctx* ctx, const float* V_in) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (!V_in) return fail(PG_EINVAL, "null input");
+    rc = ensure_stage(ctx);
+    if (rc) return rc;
+    PG_CUDA(cudaMemcpyAsync(ctx->stage_d, V_in, (size_t)ctx->kp.ncells * 4, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    cudaError_t e = pg::launch_from_rowmajor(ctx->storage, ctx->stage_d, ctx->V[ctx->cur], ctx->kp,
+                                             ctx->stream);
+    ctx->launches += 1;
+    if (e != cudaSuccess) return fail(PG_ECUDA, "from_rowmajor");
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PG_OK;
+}
+
+int pg_sweep(pg_ctx* ctx, int32_t phase, int32_t kernel, double* delta, double* maxnorm,
+             int16_t* argmin_out) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    int k = 0;
+    rc = pick_kernel(ctx, kernel, &k);
+    if (rc) return rc;
+    if (argmin_out && !ctx->argmin_d)
+        PG_CUDA(cudaMalloc(&ctx->argmin_d, (size_t)ctx->kp.ncells * sizeof(int16_t)));
+    rc = sweep_async(ctx, k, phase, false, argmin_out ? ctx->argmin_d : nullptr, false);
+    if (rc) return rc;
+    double d = 0, dm = 0;
+    rc = read_residual(ctx, &d, &dm);
+    if (rc) return rc;
+    if (delta) *delta = d;
+    if (maxnorm) *maxnorm = dm;
+    if (argmin_out) {
+        PG_CUDA(cudaMemcpyAsync(argmin_out, ctx->argmin_d, (size_t)ctx->kp.ncells * sizeof(int16_t),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return PG_OK;
+}
+
+int pg_escape_sweep(pg_ctx* ctx, int32_t phase, double* delta) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    rc = sweep_async(ctx, PG_KERNEL_CELLFORM, phase, true, nullptr, false);
+    if (rc) return rc;
+    double d = 0, dm = 0;
+    rc = read_residual(ctx, &d, &dm);
+    if (rc) return rc;
+    if (delta) *delta = d;
+    return PG_OK;
+}
+
+int pg_solve_escape(pg_ctx* ctx, int32_t iters, double tol, pg_solve_result* res,
+                    pg_progress_cb cb, void* user) {
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    int32_t done = 0;
+    double d = INFINITY, dm = INFINITY, kms = 0.0;
+    bool conv = false;
+    rc = iterate(ctx, PG_KERNEL_CELLFORM, true, iters, tol, PG_STOP_L1_QUIET, false, 0, 0, cb,
+                 user, &done, &d, &dm, &kms, &conv);
+    if (rc) return rc;
+    if (res) {
+        std::memset(res, 0, sizeof(*res));
+        res->iterations = done;
+        res->last_delta = d;
+        res->last_maxnorm = dm;
+        res->kernel_ms = kms;
+        res->cell_controls = (int64_t)done * ctx->kp.ncells * ctx->kp.nctl;
+        res->elapsed_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return PG_OK;
+}
+
+int pg_encode(pg_ctx* ctx, int32_t dtype, double scale, double escape_scale, int64_t lo,
+              int64_t n, uint8_t* out, int64_t* reached, int64_t* escaped) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (dtype < PG_DTYPE_U8 || dtype > PG_DTYPE_F32) return fail(PG_EINVAL, "unknown dtype");
+    if (lo < 0 || n < 0 || lo + n > ctx->kp.ncells) return fail(PG_EINVAL, "range outside the grid");
+    if (n == 0) {
+        if (reached) *reached = 0;
+        if (escaped) *escaped = 0;
+        return PG_OK;
+    }
+    if (!out) return fail(PG_EINVAL, "null output");
+    if ((dtype == PG_DTYPE_U8 || dtype == PG_DTYPE_U16) && !(scale > 0.0))
+        return fail(PG_EINVAL, "scale must be positive");
+    const size_t eb = dtype == PG_DTYPE_U8 ? 1 : (dtype == PG_DTYPE_F32 ? 4 : 2);
+    const size_t need = (size_t)n * eb;
+    if (ctx->enc_cap < need) {
+        if (ctx->enc_d) cudaFree(ctx->enc_d);
+        ctx->enc_d = nullptr;
+        ctx->enc_cap = 0;
+        PG_CUDA(cudaMalloc(&ctx->enc_d, need));
+        ctx->enc_cap = need;
+    }
+    PG_CUDA(cudaMemsetAsync(ctx->counts_d, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    cudaError_t e = pg::launch_encode(ctx->storage, ctx->V[ctx->cur], ctx->kp, dtype, scale,
+                                      escape_scale, lo, n, ctx->enc_d, ctx->counts_d, ctx->stream);
+    ctx->launches += 1;
+    if (e != cudaSuccess) return fail(PG_ECUDA, "encode launch");
+    unsigned long long cnt[2] = {0, 0};
+    PG_CUDA(cudaMemcpyAsync(out, ctx->enc_d, need, cudaMemcpyDeviceToHost, ctx->stream));
+    PG_CUDA(cudaMemcpyAsync(cnt, ctx->counts_d, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (reached) *reached = (int64_t)cnt[0];
+    if (escaped) *escaped = (int64_t)cnt[1];
+    return PG_OK;
+}
+
+int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
+                   double* ms_per_sweep) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (steps < 1 || warmup < 0) return fail(PG_EINVAL, "steps must be >= 1");
+    int k = 0;
+    rc = pick_kernel(ctx, kernel, &k);
+    if (rc) return rc;
+    for (int32_t i = 0; i < warmup; ++i) {
+        rc = sweep_async(ctx, k, i, false, nullptr, false);
+        if (rc) return rc;
+    }
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    PG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int32_t i = 0; i < steps; ++i) {
+        rc = sweep_async(ctx, k, warmup + i, false, nullptr, false);
+        if (rc) return rc;
+    }
+    PG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    PG_CUDA(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.0f;
+    PG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (ms_per_sweep) *ms_per_sweep = (double)ms / steps;
+    return PG_OK;
+}
+
+int pg_launch_count(pg_ctx* ctx, int64_t* launches) {
+    if (!ctx || !launches) return fail(PG_EINVAL, "null argument");
+    *launches = ctx->launches;
+    return PG_OK;
+}
+
+int pg_solve_value(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                   const uint8_t* occ, const int64_t* tidx, int64_t ntidx, const float* ctl,
+                   int32_t nctl, int32_t iters, double tol, const pg_solve_opts* opts,
+                   float* V_out, pg_solve_result* res, pg_progress_cb cb, void* user) {
+    pg_solve_opts o;
+    if (opts) o = *opts;
+    else pg_default_opts(&o);
+    int rc = pg_load_problem(ctx, g, m, p, occ, ctl, nctl, o.storage);
+    if (rc) return rc;
+    rc = pg_solve(ctx, tidx, ntidx, iters, tol, &o, res, cb, user);
+    if (rc) return rc;
+    if (V_out) return pg_get_value(ctx, V_out);
+    return PG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1055 @@
+// pg_kernels.cu -- the sweep kernels of the B200 value-iteration solver.
+//
+// Two sweep kernels compute the same Jacobi update V' = min(V, T V):
+//
+//   k_cellform  one thread per cell running the reference's whole
+//               cell_update (PeregrineSolver.jl:1205-1344): every scheme
+//               option, the escape views, the Int8 warm-start policy.
+//               Bit-identical to the CPU restatement.
+//
+//   k_stencil   the plain scheme (full control scan, one horizon, fixed
+//               probes, 64-corner multilinear) reorganised around position
+//               invariance: nothing in the dynamics reads x or y
+//               (solver/src/Tiles.jl:94-97), so for a fixed (h, vx, vy, w)
+//               plane and control the successor's heading/velocity corners,
+//               their weights, the probe heading bins and the per-substep
+//               position increments are the same for every (x, y) cell.
+//               A block integrates each control ONCE for its plane, stages
+//               the result in shared memory, and its threads then only
+//               replay the position increments (so the probe cells and
+//               envelope tests round exactly as the reference does) and
+//               gather the 64 corners.  EXACT=true keeps the reference's
+//               weight products and summation order (bit-identical to the
+//               CPU restatement); EXACT=false lets the compiler fuse the
+//               interpolation into FMAs.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pg_device.cuh"
+#include "pg_kernels.h"
+
+namespace pg {
+
+template <> struct Conv<__half> {
+    static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
+    static __device__ __forceinline__ float val(__half v) { return __half2float(v); }
+    template <typename T> static __device__ __forceinline__ __half st(T v) {
+        return __float2half_rn((float)v);
+    }
+};
+template <> struct Conv<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(const __nv_bfloat16* p) {
+        return __bfloat162float(__ldg(p));
+    }
+    static __device__ __forceinline__ float val(__nv_bfloat16 v) { return __bfloat162float(v); }
+    template <typename T> static __device__ __forceinline__ __nv_bfloat16 st(T v) {
+        return __float2bfloat16_rn((float)v);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// small utilities
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ Layout make_layout(const KParams& kp) {
+    Layout L;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) L.n[k] = kp.g.n[k];
+    L.P = kp.P;
+    L.nplanes = kp.nplanes;
+    return L;
+}
+
+// Deterministic block reduction of (sum, max) into per-block partials.
+__device__ __forceinline__ void block_partial(double s, double m, double* part_sum,
+                                              double* part_max) {
+    __shared__ double ws[32], wm[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { ws[wid] = s; wm[wid] = m; }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        s = lane < nw ? ws[lane] : 0.0;
+        m = lane < nw ? wm[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, o);
+            m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        }
+        if (lane == 0) { part_sum[blockIdx.x] = s; part_max[blockIdx.x] = m; }
+    }
+}
+
+// One block sums the partials in a fixed order: thread t takes t, t+1024, ...
+__global__ void k_reduce_parts(const double* part_sum, const double* part_max, int64_t n,
+                               double* out) {
+    __shared__ double ss[1024], sm[1024];
+    double s = 0.0, m = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        s += part_sum[i];
+        m = fmax(m, part_max[i]);
+    }
+    ss[threadIdx.x] = s;
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            ss[threadIdx.x] += ss[threadIdx.x + w];
+            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = ss[0]; out[1] = sm[0]; }
+}
+
+template <typename S>
+__global__ void k_fill(S* V, int64_t n, float v) {
+    const S sv = Conv<S>::st(v);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        V[i] = sv;
+}
+
+// V[dev(tidx)] = 0 for every seed (Run.jl:1438, 1464).  tidx is row-major.
+template <typename S>
+__global__ void k_seed(S* V, const int64_t* tidx, int64_t nt, KParams kp) {
+    const Layout L = make_layout(kp);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nt;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = tidx[t];
+        int32_t i[6];
+        for (int k = 5; k >= 1; --k) { i[k] = (int32_t)(r % L.n[k]); r /= L.n[k]; }
+        i[0] = (int32_t)r;
+        V[L.dev(i[0], i[1], i[2], i[3], i[4], i[5])] = Conv<S>::st(0.0f);
+    }
+}
+
+// Row-major float <-> device layout.
+template <typename S>
+__global__ void k_to_rowmajor(const S* V, float* out, KParams kp) {
+    const Layout L = make_layout(kp);
+    for (int64_t r0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r0 < kp.ncells;
+         r0 += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = r0;
+        int32_t i[6];
+        for (int k = 5; k >= 1; --k) { i[k] = (int32_t)(r % L.n[k]); r /= L.n[k]; }
+        i[0] = (int32_t)r;
+        out[r0] = (float)Conv<S>::ld(V + L.dev(i[0], i[1], i[2], i[3], i[4], i[5]));
+    }
+}
+
+template <typename S>
+__global__ void k_from_rowmajor(const float* in, S* V, KParams kp) {
+    const Layout L = make_layout(kp);
+    for (int64_t r0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r0 < kp.ncells;
+         r0 += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = r0;
+        int32_t i[6];
+        for (int k = 5; k >= 1; --k) { i[k] = (int32_t)(r % L.n[k]); r /= L.n[k]; }
+        i[0] = (int32_t)r;
+        V[L.dev(i[0], i[1], i[2], i[3], i[4], i[5])] = Conv<S>::st(in[r0]);
+    }
+}
+
+// Convert between storages of the same layout (16-bit phase -> FP32 polish).
+template <typename SI, typename SO>
+__global__ void k_convert(const SI* in, SO* out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = Conv<SO>::st(Conv<SI>::ld(in + i));
+}
+
+// ---------------------------------------------------------------------------
+// The reference's backup, one cell per thread
+// ---------------------------------------------------------------------------
+
+// V as cell_update reads it: plain, or through EscapeView
+// (PeregrineSolver.jl:807-824).
+template <typename T, typename S> struct VView {
+    const S* V;
+    const uint8_t* occ;
+    Layout L;
+    T cap;
+    bool esc;
+    bool ignore;
+    __device__ __forceinline__ T get(int32_t j1, int32_t j2, int32_t j3, int32_t j4, int32_t j5,
+                                     int32_t j6) const {
+        if (esc && !ignore && occ[L.occ(j1, j2, j3)]) return cap;
+        T v = (T)Conv<S>::ld(V + L.dev(j1, j2, j3, j4, j5, j6));
+        if (!esc) return v;
+        return v < (T)0 ? -v : (v < cap ? (T)0 : cap);
+    }
+};
+
+// interp (PeregrineSolver.jl:399-466)
+template <typename T, typename S>
+__device__ T interp_ml(const VView<T, S>& vv, const GridT<T>& g, const State6<T>& s, bool nearest,
+                       T cap, bool vclamp) {
+    typedef Ar<T> R;
+    T f1 = R::div(R::sub(s.x, g.lo[0]), g.step[0]);
+    T f2 = R::div(R::sub(s.y, g.lo[1]), g.step[1]);
+    T n3 = (T)g.n[2];
+    T f3 = R::div(R::sub(s.h, g.lo[2]), g.step[2]);
+    f3 = R::sub(f3, R::mul(R::floor_(R::div(f3, n3)), n3));
+    T f4 = R::div(R::sub(s.vx, g.lo[3]), g.step[3]);
+    T f5 = R::div(R::sub(s.vy, g.lo[4]), g.step[4]);
+    T f6 = R::div(R::sub(s.w, g.lo[5]), g.step[5]);
+    if (!(finite_(f1) && finite_(f2) && finite_(f3) && finite_(f4) && finite_(f5) && finite_(f6)))
+        return cap;
+    if (f1 < (T)0 || f1 > (T)(g.n[0] - 1)) return cap;
+    if (f2 < (T)0 || f2 > (T)(g.n[1] - 1)) return cap;
+    if (vclamp) {
+        f4 = jclamp(f4, (T)0, (T)(g.n[3] - 1));
+        f5 = jclamp(f5, (T)0, (T)(g.n[4] - 1));
+        f6 = jclamp(f6, (T)0, (T)(g.n[5] - 1));
+    } else {
+        if (f4 < (T)0 || f4 > (T)(g.n[3] - 1)) return cap;
+        if (f5 < (T)0 || f5 > (T)(g.n[4] - 1)) return cap;
+        if (f6 < (T)0 || f6 > (T)(g.n[5] - 1)) return cap;
+    }
+    if (nearest) {
+        int32_t i1 = (int32_t)R::rint_(f1), i2 = (int32_t)R::rint_(f2);
+        int32_t i3 = ((int32_t)R::rint_(f3)) % g.n[2];
+        int32_t i4 = (int32_t)R::rint_(f4), i5 = (int32_t)R::rint_(f5);
+        int32_t i6 = (int32_t)R::rint_(f6);
+        return vv.get(i1, i2, i3, i4, i5, i6);
+    }
+    T b[6] = {R::floor_(f1), R::floor_(f2), R::floor_(f3), R::floor_(f4), R::floor_(f5),
+              R::floor_(f6)};
+    T t[6] = {R::sub(f1, b[0]), R::sub(f2, b[1]), R::sub(f3, b[2]),
+              R::sub(f4, b[3]), R::sub(f5, b[4]), R::sub(f6, b[5])};
+    int32_t i[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) i[k] = (int32_t)b[k];
+    T acc = (T)0;
+    for (int d = 0; d < 64; ++d) {
+        int c[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) c[k] = (d >> k) & 1;
+        T wgt = c[0] ? t[0] : R::sub((T)1, t[0]);
+#pragma unroll
+        for (int k = 1; k < 6; ++k) wgt = R::mul(wgt, c[k] ? t[k] : R::sub((T)1, t[k]));
+        if (wgt == (T)0) continue;
+        int32_t j1 = min(i[0] + c[0], g.n[0] - 1);
+        int32_t j2 = min(i[1] + c[1], g.n[1] - 1);
+        int32_t j3 = (i[2] + c[2]) % g.n[2];
+        int32_t j4 = min(i[3] + c[3], g.n[3] - 1);
+        int32_t j5 = min(i[4] + c[4], g.n[4] - 1);
+        int32_t j6 = min(i[5] + c[5], g.n[5] - 1);
+        acc = R::add(acc, R::mul(wgt, vv.get(j1, j2, j3, j4, j5, j6)));
+    }
+    return jmin(acc, cap);
+}
+
+template <typename T>
+__device__ __forceinline__ void cmpx(T& ta, int32_t& ka, T& tb, int32_t& kb) {
+    if (!(ta >= tb)) {
+        T t = ta; ta = tb; tb = t;
+        int32_t k = ka; ka = kb; kb = k;
+    }
+}
+
+// interp_kuhn (PeregrineSolver.jl:571-665), value only
+template <typename T, typename S>
+__device__ T interp_kuhn(const VView<T, S>& vv, const GridT<T>& g, const State6<T>& s, T cap,
+                         bool vclamp) {
+    typedef Ar<T> R;
+    T f1 = R::div(R::sub(s.x, g.lo[0]), g.step[0]);
+    T f2 = R::div(R::sub(s.y, g.lo[1]), g.step[1]);
+    T n3 = (T)g.n[2];
+    T f3 = R::div(R::sub(s.h, g.lo[2]), g.step[2]);
+    f3 = R::sub(f3, R::mul(R::floor_(R::div(f3, n3)), n3));
+    T f4 = R::div(R::sub(s.vx, g.lo[3]), g.step[3]);
+    T f5 = R::div(R::sub(s.vy, g.lo[4]), g.step[4]);
+    T f6 = R::div(R::sub(s.w, g.lo[5]), g.step[5]);
+    if (!(finite_(f1) && finite_(f2) && finite_(f3) && finite_(f4) && finite_(f5) && finite_(f6)))
+        return cap;
+    if (f1 < (T)0 || f1 > (T)(g.n[0] - 1)) return cap;
+    if (f2 < (T)0 || f2 > (T)(g.n[1] - 1)) return cap;
+    if (vclamp) {
+        f4 = jclamp(f4, (T)0, (T)(g.n[3] - 1));
+        f5 = jclamp(f5, (T)0, (T)(g.n[4] - 1));
+        f6 = jclamp(f6, (T)0, (T)(g.n[5] - 1));
+    } else {
+        if (f4 < (T)0 || f4 > (T)(g.n[3] - 1)) return cap;
+        if (f5 < (T)0 || f5 > (T)(g.n[4] - 1)) return cap;
+        if (f6 < (T)0 || f6 > (T)(g.n[5] - 1)) return cap;
+    }
+    T b1 = R::floor_(f1), b2 = R::floor_(f2), b3 = R::floor_(f3);
+    T b4 = R::floor_(f4), b5 = R::floor_(f5), b6 = R::floor_(f6);
+    int32_t idx[6] = {(int32_t)b1, (int32_t)b2, ((int32_t)b3) % g.n[2],
+                      (int32_t)b4, (int32_t)b5, (int32_t)b6};
+    T t0 = R::sub(f1, b1), t1 = R::sub(f2, b2), t2 = R::sub(f3, b3);
+    T t3 = R::sub(f4, b4), t4 = R::sub(f5, b5), t5 = R::sub(f6, b6);
+    int32_t k0 = 1, k1 = 2, k2 = 3, k3 = 4, k4 = 5, k5 = 6;
+    cmpx(t0, k0, t5, k5);
+    cmpx(t1, k1, t3, k3);
+    cmpx(t2, k2, t4, k4);
+    cmpx(t1, k1, t2, k2);
+    cmpx(t3, k3, t4, k4);
+    cmpx(t0, k0, t3, k3);
+    cmpx(t2, k2, t5, k5);
+    cmpx(t0, k0, t1, k1);
+    cmpx(t2, k2, t3, k3);
+    cmpx(t4, k4, t5, k5);
+    cmpx(t1, k1, t2, k2);
+    cmpx(t3, k3, t4, k4);
+    const T ts[6] = {t0, t1, t2, t3, t4, t5};
+    const int32_t ks[6] = {k0, k1, k2, k3, k4, k5};
+    T v0 = vv.get(idx[0], idx[1], idx[2], idx[3], idx[4], idx[5]);
+    T acc = R::mul(R::sub((T)1, ts[0]), v0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int32_t k = ks[q];
+        if (k == 3) idx[2] = (idx[2] + 1) % g.n[2];
+        else idx[k - 1] = min(idx[k - 1] + 1, g.n[k - 1] - 1);
+        T v = vv.get(idx[0], idx[1], idx[2], idx[3], idx[4], idx[5]);
+        T wq = q < 5 ? R::sub(ts[q], ts[q + 1]) : ts[5];
+        acc = R::add(acc, R::mul(wq, v));
+    }
+    return jmin(acc, cap);
+}
+
+template <typename T, typename S>
+__device__ __forceinline__ T value_at(const VView<T, S>& vv, const GridT<T>& g, const State6<T>& s,
+                                      const pg_params& p) {
+    if (p.simplex) return interp_kuhn(vv, g, s, (T)p.cap, p.vclamp != 0);
+    return interp_ml(vv, g, s, p.nearest != 0, (T)p.cap, p.vclamp != 0);
+}
+
+// lookahead (PeregrineSolver.jl:1100-1153)
+template <typename T, typename S>
+__device__ T lookahead(const VView<T, S>& vv, const uint8_t* occ, bool occ_ignore,
+                       const GridT<T>& g, const ModelT<T>& m, const Layout& L,
+                       const State6<T>& s0, T u1, T u2, T u3, T tau, int32_t nsub,
+                       const pg_params& p) {
+    typedef Ar<T> R;
+    const T cap = (T)p.cap;
+    State6<T> ns = s0;
+    if (!integrate(m, ns, u1, u2, u3, tau, nsub, p.rk2 != 0, (T*)nullptr, (T*)nullptr))
+        return cap;  // NANSTATE: every difference below is non-finite
+    T dx = R::sub(ns.x, s0.x), dy = R::sub(ns.y, s0.y), dh = R::sub(ns.h, s0.h);
+    if (!(finite_(dx) && finite_(dy) && finite_(dh) && finite_(ns.vx) && finite_(ns.vy) &&
+          finite_(ns.w)))
+        return cap;
+    int32_t nchk = p.checks;
+    if (p.adaptive_checks) {
+        T cells_pos = R::div(R::sqrt_(R::add(R::mul(dx, dx), R::mul(dy, dy))),
+                             R::mul((T)0.5f, jmin(g.step[0], g.step[1])));
+        T cells_rot = R::div(R::abs_(dh), R::mul((T)0.5f, g.step[2]));
+        T cells = jmin(jmax(cells_pos, cells_rot), (T)1.0e4f);
+        int32_t need = (int32_t)cells + 1;
+        nchk = max(p.checks, min(need, 24));
+    }
+    const T n3f = (T)g.n[2];
+    for (int32_t sc = 1; sc <= nchk; ++sc) {
+        T a = R::div((T)sc, (T)nchk);
+        T px = R::add(s0.x, R::mul(dx, a));
+        T py = R::add(s0.y, R::mul(dy, a));
+        T ph = R::add(s0.h, R::mul(dh, a));
+        T gx = R::div(R::sub(px, g.lo[0]), g.step[0]);
+        T gy = R::div(R::sub(py, g.lo[1]), g.step[1]);
+        if (gx < (T)0 || gy < (T)0 || gx > (T)(g.n[0] - 1) || gy > (T)(g.n[1] - 1)) return cap;
+        T gh = R::div(R::sub(ph, g.lo[2]), g.step[2]);
+        gh = R::sub(gh, R::mul(R::floor_(R::div(gh, n3f)), n3f));
+        int32_t ci = (int32_t)R::rint_(gx), cj = (int32_t)R::rint_(gy);
+        int32_t ck = ((int32_t)R::rint_(gh)) % g.n[2];
+        if (!occ_ignore && occ[L.occ(ci, cj, ck)]) return cap;
+    }
+    T snh, cnh;
+    R::sincos_(ns.h, &snh, &cnh);
+    State6<T> q = ns;
+    q.vx = R::sub(R::mul(cnh, ns.vx), R::mul(snh, ns.vy));
+    q.vy = R::add(R::mul(snh, ns.vx), R::mul(cnh, ns.vy));
+    T nv = value_at(vv, g, q, p);
+    return jmin(R::add(tau, nv), cap);
+}
+
+template <typename T> __device__ __forceinline__ int8_t qpol(T v) {
+    typedef Ar<T> R;
+    return (int8_t)(int32_t)R::rint_(R::mul(jclamp(v, (T)-1, (T)1), (T)127.0f));
+}
+
+// cell_update (PeregrineSolver.jl:1205-1344).  Returns best; b[] the command.
+template <typename T, typename S>
+__device__ T cell_update(const int32_t* i, const VView<T, S>& vv, const uint8_t* occ,
+                         const int8_t* pol, int64_t pidx, const GridT<T>& g, const ModelT<T>& m,
+                         const Layout& L, const float* ctl, int32_t nctl, const pg_params& p,
+                         int32_t phase, bool esc, bool blocked, T* b) {
+    typedef Ar<T> R;
+    b[0] = b[1] = b[2] = (T)0;
+    const bool oign = esc && blocked;
+    State6<T> s;
+    s.x = axisvalue(g, 0, i[0]);
+    s.y = axisvalue(g, 1, i[1]);
+    s.h = axisvalue(g, 2, i[2]);
+    T vfx = axisvalue(g, 3, i[3]);
+    T vfy = axisvalue(g, 4, i[4]);
+    s.w = axisvalue(g, 5, i[5]);
+    T sh0, ch0;
+    R::sincos_(s.h, &sh0, &ch0);
+    s.vx = R::add(R::mul(ch0, vfx), R::mul(sh0, vfy));
+    s.vy = R::add(R::mul(-sh0, vfx), R::mul(ch0, vfy));
+    T tau0 = cfl_tau(g, m, vfx, vfy, s.w, p);
+    int32_t ns0 = substeps_for(tau0, p);
+
+    T best = lookahead(vv, occ, oign, g, m, L, s, (T)0, (T)0, (T)0, tau0, ns0, p);
+    T b1 = 0, b2 = 0, b3 = 0;
+    if (pol != nullptr && !esc) {
+        const T k127 = (T)(1.0f / 127.0f);
+        T q1 = R::mul((T)pol[3 * pidx], k127);
+        T q2 = R::mul((T)pol[3 * pidx + 1], k127);
+        T q3 = R::mul((T)pol[3 * pidx + 2], k127);
+        if (R::add(R::add(R::abs_(q1), R::abs_(q2)), R::abs_(q3)) > (T)1.0e-6f) {
+            T c = lookahead(vv, occ, oign, g, m, L, s, q1, q2, q3, tau0, ns0, p);
+            if (c < best) { best = c; b1 = q1; b2 = q2; b3 = q3; }
+        }
+    }
+    const int32_t nnc = max(nctl - 1, 1);
+    const int32_t span = p.ncoarse <= 0 ? nnc : min(p.ncoarse, nnc);
+    int32_t off = p.ncoarse <= 0 ? 0 : (int32_t)(((int64_t)phase * span) % nnc);
+    if (off < 0) off += nnc;
+    for (int32_t j = 0; j < span; ++j) {
+        int32_t k = (int32_t)(((int64_t)off + j) % nnc) + 1;
+        T u1 = (T)ctl[k], u2 = (T)ctl[k + nctl], u3 = (T)ctl[k + 2 * nctl];
+        T c = lookahead(vv, occ, oign, g, m, L, s, u1, u2, u3, tau0, ns0, p);
+        if (c < best) { best = c; b1 = u1; b2 = u2; b3 = u3; }
+    }
+    T delta = (T)p.delta0;
+    for (int32_t r = 0; r < p.rounds; ++r) {
+        for (int32_t d = 1; d <= 6; ++d) {
+            T sdl = (d % 2 == 0) ? -delta : delta;
+            T e1 = d <= 2 ? sdl : (T)0;
+            T e2 = (d == 3 || d == 4) ? sdl : (T)0;
+            T e3 = d >= 5 ? sdl : (T)0;
+            T a1 = R::add(b1, e1), a2 = R::add(b2, e2), a3 = R::add(b3, e3);
+            T sm = R::add(R::add(R::abs_(a1), R::abs_(a2)), R::abs_(a3));
+            T c1, c2, c3;
+            if (sm < (T)1.0e-6f) { c1 = c2 = c3 = (T)0; }
+            else {
+                T rr = R::div((T)1, sm);
+                c1 = R::mul(a1, rr); c2 = R::mul(a2, rr); c3 = R::mul(a3, rr);
+            }
+            if (R::add(R::add(R::abs_(c1), R::abs_(c2)), R::abs_(c3)) < (T)1.0e-6f) continue;
+            T c = lookahead(vv, occ, oign, g, m, L, s, c1, c2, c3, tau0, ns0, p);
+            if (c < best) { best = c; b1 = c1; b2 = c2; b3 = c3; }
+        }
+        delta = R::mul(delta, (T)0.5f);
+    }
+    if (p.ntau > 1) {
+        T tau = R::mul(tau0, (T)0.5f);
+        for (int32_t k = 1; k <= p.ntau; ++k) {
+            if (k != 2) {
+                T t = jmin(jmax(tau, (T)p.tau_min), (T)p.tau_max);
+                T c = lookahead(vv, occ, oign, g, m, L, s, b1, b2, b3, t, substeps_for(t, p), p);
+                if (c < best) best = c;
+            }
+            tau = R::mul(tau, (T)p.tau_ratio);
+        }
+        if (p.cfl > 0.0f) {
+            T t = jmin(jmax((T)p.dt, (T)p.tau_min), (T)p.tau_max);
+            T c = lookahead(vv, occ, oign, g, m, L, s, b1, b2, b3, t, substeps_for(t, p), p);
+            if (c < best) best = c;
+        }
+    }
+    b[0] = b1; b[1] = b2; b[2] = b3;
+    return best;
+}
+
+__device__ __forceinline__ int16_t ctl_index(const float* ctl, int32_t nctl, float u1, float u2,
+                                             float u3) {
+    for (int32_t k = 0; k < nctl; ++k)
+        if (ctl[k] == u1 && ctl[k + nctl] == u2 && ctl[k + 2 * nctl] == u3) return (int16_t)k;
+    return (int16_t)-1;
+}
+
+// Sweep (ESC=false): gpu_sweep_kernel! (Gpu.jl:5-24) as a Jacobi update.
+// Escape (ESC=true): gpu_escape_kernel! (Gpu.jl:51-67) as a Jacobi update.
+template <typename S, typename T, bool ESC>
+__global__ void __launch_bounds__(kCellThreads)
+    k_cellform(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
+               int8_t* pol, KParams kp, const float* __restrict__ ctl, double* part_sum,
+               double* part_max, int16_t* argmin) {
+    typedef Ar<T> R;
+    const Layout L = make_layout(kp);
+    GridT<T> g;
+    load_grid(g, kp.g);
+    ModelT<T> m;
+    load_model(m, kp.m);
+    const T cap = (T)kp.p.cap;
+    double dsum = 0.0, dmax = 0.0;
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx < kp.ncells) {
+        int64_t pl = idx / L.P;
+        int32_t r = (int32_t)(idx - pl * L.P);
+        int32_t i[6];
+        i[0] = r / L.n[1];
+        i[1] = r - i[0] * L.n[1];
+        i[5] = (int32_t)(pl % L.n[5]); pl /= L.n[5];
+        i[4] = (int32_t)(pl % L.n[4]); pl /= L.n[4];
+        i[3] = (int32_t)(pl % L.n[3]); pl /= L.n[3];
+        i[2] = (int32_t)pl;
+        const bool blocked = occ[L.occ(i[0], i[1], i[2])] != 0;
+        const T old = (T)Conv<S>::ld(Vin + idx);
+        S outv = Vin[idx];
+        VView<T, S> vv{Vin, occ, L, cap, ESC, blocked};
+        if (!ESC) {
+            if (blocked) {
+                if (argmin) argmin[L.rowmajor(i[0], i[1], i[2], i[3], i[4], i[5])] = -1;
+            } else {
+                T b[3];
+                T c = cell_update(i, vv, occ, pol, idx, g, m, L, ctl, kp.nctl, kp.p, kp.phase,
+                                  false, false, b);
+                if (argmin)
+                    argmin[L.rowmajor(i[0], i[1], i[2], i[3], i[4], i[5])] =
+                        ctl_index(ctl, kp.nctl, (float)b[0], (float)b[1], (float)b[2]);
+                if (c < old) {
+                    S nv = Conv<S>::template st<T>(c);
+                    T nvT = (T)Conv<S>::val(nv);
+                    outv = nv;
+                    if (pol) {
+                        pol[3 * idx] = qpol(b[0]);
+                        pol[3 * idx + 1] = qpol(b[1]);
+                        pol[3 * idx + 2] = qpol(b[2]);
+                    }
+                    double d = (double)old - (double)nvT;
+                    dsum = d;
+                    dmax = d;
+                }
+            }
+        } else {
+            // is_terminal / escape_of (PeregrineSolver.jl:860-866)
+            if (!(old >= (T)0 && old < cap)) {
+                const T e_old = old < (T)0 ? -old : cap;
+                T b[3];
+                T c = cell_update(i, vv, occ, (const int8_t*)nullptr, idx, g, m, L, ctl, kp.nctl,
+                                  kp.p, kp.phase, true, blocked, b);
+                if (c < e_old) {
+                    outv = Conv<S>::template st<T>(-c);
+                    double d = (double)e_old - (double)c;
+                    dsum = d;
+                    dmax = d;
+                }
+            }
+        }
+        Vout[idx] = outv;
+        (void)R::add;
+    }
+    block_partial(dsum, dmax, part_sum, part_max);
+}
+
+// ---------------------------------------------------------------------------
+// The plain scheme as a position-invariant stencil
+// ---------------------------------------------------------------------------
+
+// Shared-memory staging of one plane's transitions, structure of arrays
+// indexed [item][control] so a warp reading one control broadcasts.
+template <typename T> struct StencilSmem {
+    T* incx;       // [nsub][nctl]
+    T* incy;       // [nsub][nctl]
+    T* w;          // EXACT: [8][nctl] (1-t, t for h, vx, vy, w); fast: [16][nctl] products
+    T* aprobe;     // [nchk]
+    int32_t* plane;// [16][nctl] corner plane indices
+    int32_t* ck;   // [nchk][nctl] probe heading bins
+    int32_t* ok;   // [nctl]
+    T* tau;        // [nctl]
+};
+
+template <typename T, bool EXACT>
+__host__ __device__ inline size_t stencil_smem_bytes(int nctl, int nsub, int nchk) {
+    size_t nt = (size_t)(2 * nsub + (EXACT ? 8 : 16) + 1) * nctl + nchk;
+    size_t ni = (size_t)(16 + nchk + 1) * nctl;
+    return nt * sizeof(T) + ni * sizeof(int32_t) + 64;
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ StencilSmem<T> carve(unsigned char* base, int nctl, int nsub, int nchk) {
+    StencilSmem<T> s;
+    T* tp = (T*)base;
+    s.incx = tp; tp += (size_t)nsub * nctl;
+    s.incy = tp; tp += (size_t)nsub * nctl;
+    s.w = tp; tp += (size_t)(EXACT ? 8 : 16) * nctl;
+    s.tau = tp; tp += nctl;
+    s.aprobe = tp; tp += nchk;
+    int32_t* ip = (int32_t*)tp;
+    s.plane = ip; ip += 16 * nctl;
+    s.ck = ip; ip += (size_t)nchk * nctl;
+    s.ok = ip;
+    return s;
+}
+
+template <typename S, typename T, bool EXACT>
+__global__ void __launch_bounds__(kStencilThreads)
+    k_stencil(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
+              KParams kp, const float* __restrict__ ctl, double* part_sum, double* part_max,
+              int16_t* argmin) {
+    typedef Ar<T> R;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nctl = kp.nctl, nsub = kp.nsub, nchk = kp.nchk;
+    StencilSmem<T> sm = carve<T, EXACT>(smem_raw, nctl, nsub, nchk);
+    const Layout L = make_layout(kp);
+    GridT<T> g;
+    load_grid(g, kp.g);
+    const T cap = (T)kp.p.cap;
+
+    const int64_t pl = blockIdx.x / kp.tiles_x;
+    const int32_t xt = (int32_t)(blockIdx.x - pl * kp.tiles_x);
+    int32_t i3, i4, i5, i6;
+    {
+        int64_t q = pl;
+        i6 = (int32_t)(q % L.n[5]); q /= L.n[5];
+        i5 = (int32_t)(q % L.n[4]); q /= L.n[4];
+        i4 = (int32_t)(q % L.n[3]); q /= L.n[3];
+        i3 = (int32_t)q;
+    }
+
+    // Phase A: one thread per control integrates the held command from this
+    // plane's (h, v) -- the work the reference repeats for every (x, y).
+    if ((int)threadIdx.x < nchk) sm.aprobe[threadIdx.x] = R::div((T)(threadIdx.x + 1), (T)nchk);
+    for (int u = threadIdx.x; u < nctl; u += blockDim.x) {
+        ModelT<T> m;
+        load_model(m, kp.m);
+        State6<T> s;
+        s.x = g.lo[0];  // representative position: the dynamics never read it
+        s.y = g.lo[1];
+        s.h = axisvalue(g, 2, i3);
+        T vfx = axisvalue(g, 3, i4), vfy = axisvalue(g, 4, i5);
+        s.w = axisvalue(g, 5, i6);
+        T sh0, ch0;
+        R::sincos_(s.h, &sh0, &ch0);
+        s.vx = R::add(R::mul(ch0, vfx), R::mul(sh0, vfy));
+        s.vy = R::add(R::mul(-sh0, vfx), R::mul(ch0, vfy));
+        T tau0 = cfl_tau(g, m, vfx, vfy, s.w, kp.p);
+        int32_t ns = substeps_for(tau0, kp.p);
+        T incx[kStencilMaxSub], incy[kStencilMaxSub];
+        State6<T> ns6 = s;
+        bool ok = ns <= nsub &&
+                  integrate(m, ns6, (T)ctl[u], (T)ctl[u + nctl], (T)ctl[u + 2 * nctl], tau0, ns,
+                            kp.p.rk2 != 0, incx, incy);
+        for (int k = 0; k < nsub; ++k) {
+            sm.incx[k * nctl + u] = k < ns ? incx[k] : (T)0;
+            sm.incy[k * nctl + u] = k < ns ? incy[k] : (T)0;
+        }
+        sm.tau[u] = tau0;
+        T dh = R::sub(ns6.h, s.h);
+        ok = ok && finite_(R::sub(ns6.x, s.x)) && finite_(R::sub(ns6.y, s.y)) && finite_(dh) &&
+             finite_(ns6.vx) && finite_(ns6.vy) && finite_(ns6.w);
+        const T n3f = (T)g.n[2];
+        for (int sc = 0; sc < nchk; ++sc) {
+            int32_t ck = 0;
+            if (ok) {
+                T a = R::div((T)(sc + 1), (T)nchk);
+                T ph = R::add(s.h, R::mul(dh, a));
+                T gh = R::div(R::sub(ph, g.lo[2]), g.step[2]);
+                gh = R::sub(gh, R::mul(R::floor_(R::div(gh, n3f)), n3f));
+                ck = ((int32_t)R::rint_(gh)) % g.n[2];
+            }
+            sm.ck[sc * nctl + u] = ck;
+        }
+        int32_t jb[4] = {0, 0, 0, 0};
+        T tt[4] = {0, 0, 0, 0};
+        if (ok) {
+            T snh, cnh;
+            R::sincos_(ns6.h, &snh, &cnh);
+            T nvfx = R::sub(R::mul(cnh, ns6.vx), R::mul(snh, ns6.vy));
+            T nvfy = R::add(R::mul(snh, ns6.vx), R::mul(cnh, ns6.vy));
+            T f3 = R::div(R::sub(ns6.h, g.lo[2]), g.step[2]);
+            f3 = R::sub(f3, R::mul(R::floor_(R::div(f3, n3f)), n3f));
+            T f[4] = {f3, R::div(R::sub(nvfx, g.lo[3]), g.step[3]),
+                      R::div(R::sub(nvfy, g.lo[4]), g.step[4]),
+                      R::div(R::sub(ns6.w, g.lo[5]), g.step[5])};
+            ok = finite_(f[0]) && finite_(f[1]) && finite_(f[2]) && finite_(f[3]);
+            if (ok) {
+                for (int k = 1; k < 4; ++k) {
+                    T hi = (T)(g.n[2 + k] - 1);
+                    if (kp.p.vclamp) f[k] = jclamp(f[k], (T)0, hi);
+                    else if (f[k] < (T)0 || f[k] > hi) ok = false;
+                }
+            }
+            if (ok) {
+                for (int k = 0; k < 4; ++k) {
+                    T b = R::floor_(f[k]);
+                    tt[k] = R::sub(f[k], b);
+                    jb[k] = (int32_t)b;
+                }
+            }
+        }
+        sm.ok[u] = ok ? 1 : 0;
+        for (int c = 0; c < 16; ++c) {
+            const int c3 = c & 1, c4 = (c >> 1) & 1, c5 = (c >> 2) & 1, c6 = (c >> 3) & 1;
+            int32_t j3 = (jb[0] + c3) % g.n[2];
+            int32_t j4 = min(jb[1] + c4, g.n[3] - 1);
+            int32_t j5 = min(jb[2] + c5, g.n[4] - 1);
+            int32_t j6 = min(jb[3] + c6, g.n[5] - 1);
+            sm.plane[c * nctl + u] = ((j3 * g.n[3] + j4) * g.n[4] + j5) * g.n[5] + j6;
+            if (!EXACT) {
+                T w3 = c3 ? tt[0] : (T)1 - tt[0];
+                T w4 = c4 ? tt[1] : (T)1 - tt[1];
+                T w5 = c5 ? tt[2] : (T)1 - tt[2];
+                T w6 = c6 ? tt[3] : (T)1 - tt[3];
+                sm.w[c * nctl + u] = w3 * w4 * w5 * w6;
+            }
+        }
+        if (EXACT) {
+            for (int k = 0; k < 4; ++k) {
+                sm.w[(2 * k) * nctl + u] = R::sub((T)1, tt[k]);
+                sm.w[(2 * k + 1) * nctl + u] = tt[k];
+            }
+        }
+    }
+    __syncthreads();
+
+    // Phase B: every (x, y) cell of this tile scans all controls.
+    const int32_t n1 = L.n[0], n2 = L.n[1];
+    const int32_t x0 = (int32_t)xt * kp.tile_x;
+    const int32_t x1 = min(x0 + kp.tile_x, n1);
+    const int32_t ncell_tile = (x1 - x0) * n2;
+    const T lo0 = g.lo[0], lo1 = g.lo[1], st0 = g.step[0], st1 = g.step[1];
+    const T hx = (T)(n1 - 1), hy = (T)(n2 - 1);
+    const int64_t P = L.P;
+    const S* Vbase = Vin;
+    double dsum = 0.0, dmax = 0.0;
+    for (int c = threadIdx.x; c < ncell_tile; c += blockDim.x) {
+        const int32_t i1 = x0 + c / n2;
+        const int32_t i2 = c - (i1 - x0) * n2;
+        const int64_t didx = pl * P + (int64_t)i1 * n2 + i2;
+        const T old = (T)Conv<S>::ld(Vin + didx);
+        if (occ[L.occ(i1, i2, i3)]) {
+            Vout[didx] = Vin[didx];
+            if (argmin) argmin[L.rowmajor(i1, i2, i3, i4, i5, i6)] = -1;
+            continue;
+        }
+        const T x = axisvalue(g, 0, i1), y = axisvalue(g, 1, i2);
+        T best = cap;
+        int bk = 0;
+        for (int u = 0; u < nctl; ++u) {
+            T cval = cap;
+            if (sm.ok[u]) {
+                T xn = x, yn = y;
+                for (int k = 0; k < nsub; ++k) {
+                    xn = R::add(xn, sm.incx[k * nctl + u]);
+                    yn = R::add(yn, sm.incy[k * nctl + u]);
+                }
+                const T dx = R::sub(xn, x), dy = R::sub(yn, y);
+                bool hit = false;
+                for (int sc = 0; sc < nchk; ++sc) {
+                    const T a = sm.aprobe[sc];
+                    const T gx = R::div(R::sub(R::add(x, R::mul(dx, a)), lo0), st0);
+                    const T gy = R::div(R::sub(R::add(y, R::mul(dy, a)), lo1), st1);
+                    if (gx < (T)0 || gy < (T)0 || gx > hx || gy > hy) { hit = true; break; }
+                    const int32_t ci = (int32_t)R::rint_(gx), cj = (int32_t)R::rint_(gy);
+                    if (occ[L.occ(ci, cj, sm.ck[sc * nctl + u])]) { hit = true; break; }
+                }
+                if (!hit) {
+                    const T f1 = R::div(R::sub(xn, lo0), st0);
+                    const T f2 = R::div(R::sub(yn, lo1), st1);
+                    if (!(f1 < (T)0 || f1 > hx || f2 < (T)0 || f2 > hy)) {
+                        const T b1 = R::floor_(f1), b2 = R::floor_(f2);
+                        const T t1 = R::sub(f1, b1), t2 = R::sub(f2, b2);
+                        const int32_t j1 = (int32_t)b1, j2 = (int32_t)b2;
+                        const int32_t j1p = min(j1 + 1, n1 - 1), j2p = min(j2 + 1, n2 - 1);
+                        const int64_t o00 = (int64_t)j1 * n2 + j2, o01 = (int64_t)j1 * n2 + j2p;
+                        const int64_t o10 = (int64_t)j1p * n2 + j2, o11 = (int64_t)j1p * n2 + j2p;
+                        T acc = (T)0;
+                        if (EXACT) {
+                            // the reference's left-to-right weight products, corners
+                            // in its order (x fastest), one rounding per operation
+                            const T w1[2] = {R::sub((T)1, t1), t1};
+                            const T w2[2] = {R::sub((T)1, t2), t2};
+                            T p12[4];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) p12[q] = R::mul(w1[q & 1], w2[q >> 1]);
+                            for (int hc = 0; hc < 16; ++hc) {
+                                const int c3 = hc & 1, c4 = (hc >> 1) & 1, c5 = (hc >> 2) & 1,
+                                          c6 = (hc >> 3) & 1;
+                                const T w3 = sm.w[(0 + c3) * nctl + u];
+                                const T w4 = sm.w[(2 + c4) * nctl + u];
+                                const T w5 = sm.w[(4 + c5) * nctl + u];
+                                const T w6 = sm.w[(6 + c6) * nctl + u];
+                                const S* Vp = Vbase + (int64_t)sm.plane[hc * nctl + u] * P;
+                                const T v[4] = {(T)Conv<S>::ld(Vp + o00), (T)Conv<S>::ld(Vp + o10),
+                                                (T)Conv<S>::ld(Vp + o01), (T)Conv<S>::ld(Vp + o11)};
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    T wgt = R::mul(R::mul(R::mul(R::mul(p12[q], w3), w4), w5), w6);
+                                    if (wgt != (T)0) acc = R::add(acc, R::mul(wgt, v[q]));
+                                }
+                            }
+                        } else {
+                            const T u1 = (T)1 - t1, u2 = (T)1 - t2;
+                            for (int hc = 0; hc < 16; ++hc) {
+                                const S* Vp = Vbase + (int64_t)sm.plane[hc * nctl + u] * P;
+                                const T v00 = (T)Conv<S>::ld(Vp + o00), v01 = (T)Conv<S>::ld(Vp + o01);
+                                const T v10 = (T)Conv<S>::ld(Vp + o10), v11 = (T)Conv<S>::ld(Vp + o11);
+                                const T sxy = u1 * (u2 * v00 + t2 * v01) + t1 * (u2 * v10 + t2 * v11);
+                                acc += sm.w[hc * nctl + u] * sxy;
+                            }
+                        }
+                        const T nv = jmin(acc, cap);
+                        cval = jmin(R::add(sm.tau[u], nv), cap);
+                    }
+                }
+            }
+            if (u == 0) { best = cval; bk = 0; }
+            else if (cval < best) { best = cval; bk = u; }
+        }
+        if (argmin) argmin[L.rowmajor(i1, i2, i3, i4, i5, i6)] = (int16_t)bk;
+        if (best < old) {
+            const S nv = Conv<S>::template st<T>(best);
+            const T nvT = (T)Conv<S>::val(nv);
+            Vout[didx] = nv;
+            const double d = (double)old - (double)nvT;
+            dsum += d;
+            dmax = fmax(dmax, d);
+        } else {
+            Vout[didx] = Vin[didx];
+        }
+    }
+    block_partial(dsum, dmax, part_sum, part_max);
+}
+
+// ---------------------------------------------------------------------------
+// Encoding (encode_into!, Pipeline.jl:698-780), from the device layout into
+// a row-major range.
+// ---------------------------------------------------------------------------
+template <typename S>
+__global__ void k_encode(const S* V, KParams kp, int32_t dtype, double scale, double escape_scale,
+                         int64_t lo, int64_t n, uint8_t* out, unsigned long long* counts) {
+    const Layout L = make_layout(kp);
+    const float cap = kp.p.cap;
+    const uint32_t sentinel = dtype == PG_DTYPE_U8 ? 0xffu : 0xffffu;
+    const uint32_t base = dtype == PG_DTYPE_U8 ? 0xe0u : (dtype == PG_DTYPE_U16 ? 0xfc00u : 0u);
+    const int64_t codes = base == 0 ? 0 : (int64_t)sentinel - (int64_t)base;
+    const bool hasband = escape_scale > 0.0 && base != 0;
+    const uint32_t ebase = hasband ? base : sentinel;
+    const uint32_t ecodes = (uint32_t)(codes > 1 ? codes : 1);
+    const double einv = escape_scale > 0.0 ? 1.0 / escape_scale : 0.0;
+    unsigned long long nr = 0, ne = 0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = lo + t;
+        int32_t i[6];
+        for (int k = 5; k >= 1; --k) { i[k] = (int32_t)(r % L.n[k]); r /= L.n[k]; }
+        i[0] = (int32_t)r;
+        const float v = (float)Conv<S>::ld(V + L.dev(i[0], i[1], i[2], i[3], i[4], i[5]));
+        const bool isesc = v < 0.0f && isfinite(v);
+        const bool unre = v >= cap || isinf(v) || isnan(v);
+        if (dtype == PG_DTYPE_F32 || dtype == PG_DTYPE_F16) {
+            const bool u = !isesc && unre;
+            nr += (!isesc && !u);
+            ne += isesc;
+            if (dtype == PG_DTYPE_F32) {
+                const uint32_t bits = u ? 0x7fc00000u : __float_as_uint(v);
+                reinterpret_cast<uint32_t*>(out)[t] = bits;
+            } else {
+                const uint16_t hb = u ? (uint16_t)0x7e00u : __half_as_ushort(__float2half_rn(v));
+                reinterpret_cast<uint16_t*>(out)[t] = hb;
+            }
+            continue;
+        }
+        uint32_t code;
+        if (isesc) {
+            ++ne;
+            const double e = -(double)v;
+            const double q = __dsqrt_rn(__dmul_rn(e > 0.0 ? e : 0.0, einv));
+            const uint32_t rq = (uint32_t)rint(q);
+            code = ebase + (rq < ecodes - 1u ? rq : ecodes - 1u);
+        } else if (unre) {
+            code = sentinel;
+        } else {
+            ++nr;
+            const uint32_t rr = (uint32_t)rint(__ddiv_rn((double)v, scale));
+            code = rr >= ebase ? sentinel : rr;
+        }
+        if (dtype == PG_DTYPE_U8) out[t] = (uint8_t)code;
+        else reinterpret_cast<uint16_t*>(out)[t] = (uint16_t)code;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nr += __shfl_down_sync(0xffffffffu, nr, o);
+        ne += __shfl_down_sync(0xffffffffu, ne, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&counts[0], nr);
+        atomicAdd(&counts[1], ne);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers
+// ---------------------------------------------------------------------------
+static inline int grid_for(int64_t n, int threads) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b > (int64_t)148 * 64) b = (int64_t)148 * 64;
+    return (int)(b < 1 ? 1 : b);
+}
+
+template <typename S>
+static cudaError_t fill_seed_t(void* V, const KParams& kp, const int64_t* tidx_dev, int64_t nt,
+                               cudaStream_t st) {
+    k_fill<S><<<grid_for(kp.ncells, 256), 256, 0, st>>>((S*)V, kp.ncells, kp.p.cap);
+    if (nt > 0) k_seed<S><<<grid_for(nt, 256), 256, 0, st>>>((S*)V, tidx_dev, nt, kp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_seed(int storage, void* V, const KParams& kp, const int64_t* tidx_dev,
+                             int64_t nt, cudaStream_t st) {
+    switch (storage) {
+        case PG_STORE_F32: return fill_seed_t<float>(V, kp, tidx_dev, nt, st);
+        case PG_STORE_F16: return fill_seed_t<__half>(V, kp, tidx_dev, nt, st);
+        case PG_STORE_BF16: return fill_seed_t<__nv_bfloat16>(V, kp, tidx_dev, nt, st);
+        case PG_STORE_F64: return fill_seed_t<double>(V, kp, tidx_dev, nt, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_seed_only(int storage, void* V, const KParams& kp, const int64_t* tidx_dev,
+                             int64_t nt, cudaStream_t st) {
+    if (nt <= 0) return cudaSuccess;
+    switch (storage) {
+        case PG_STORE_F32: k_seed<float><<<grid_for(nt, 256), 256, 0, st>>>((float*)V, tidx_dev, nt, kp); break;
+        case PG_STORE_F16: k_seed<__half><<<grid_for(nt, 256), 256, 0, st>>>((__half*)V, tidx_dev, nt, kp); break;
+        case PG_STORE_BF16: k_seed<__nv_bfloat16><<<grid_for(nt, 256), 256, 0, st>>>((__nv_bfloat16*)V, tidx_dev, nt, kp); break;
+        case PG_STORE_F64: k_seed<double><<<grid_for(nt, 256), 256, 0, st>>>((double*)V, tidx_dev, nt, kp); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_rowmajor(int storage, const void* V, float* out, const KParams& kp,
+                               cudaStream_t st) {
+    const int b = grid_for(kp.ncells, 256);
+    switch (storage) {
+        case PG_STORE_F32: k_to_rowmajor<float><<<b, 256, 0, st>>>((const float*)V, out, kp); break;
+        case PG_STORE_F16: k_to_rowmajor<__half><<<b, 256, 0, st>>>((const __half*)V, out, kp); break;
+        case PG_STORE_BF16: k_to_rowmajor<__nv_bfloat16><<<b, 256, 0, st>>>((const __nv_bfloat16*)V, out, kp); break;
+        case PG_STORE_F64: k_to_rowmajor<double><<<b, 256, 0, st>>>((const double*)V, out, kp); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_from_rowmajor(int storage, const float* in, void* V, const KParams& kp,
+                                 cudaStream_t st) {
+    const int b = grid_for(kp.ncells, 256);
+    switch (storage) {
+        case PG_STORE_F32: k_from_rowmajor<float><<<b, 256, 0, st>>>(in, (float*)V, kp); break;
+        case PG_STORE_F16: k_from_rowmajor<__half><<<b, 256, 0, st>>>(in, (__half*)V, kp); break;
+        case PG_STORE_BF16: k_from_rowmajor<__nv_bfloat16><<<b, 256, 0, st>>>(in, (__nv_bfloat16*)V, kp); break;
+        case PG_STORE_F64: k_from_rowmajor<double><<<b, 256, 0, st>>>(in, (double*)V, kp); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert_to_f32(int storage, const void* in, float* out, int64_t n,
+                                  cudaStream_t st) {
+    const int b = grid_for(n, 256);
+    switch (storage) {
+        case PG_STORE_F16: k_convert<__half, float><<<b, 256, 0, st>>>((const __half*)in, out, n); break;
+        case PG_STORE_BF16: k_convert<__nv_bfloat16, float><<<b, 256, 0, st>>>((const __nv_bfloat16*)in, out, n); break;
+        case PG_STORE_F32: return cudaMemcpyAsync(out, in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename S, typename T, bool ESC>
+static cudaError_t cellform_t(const void* Vin, void* Vout, const uint8_t* occ, int8_t* pol,
+                              const KParams& kp, const float* ctl, const SweepBufs& sb,
+                              int16_t* argmin, cudaStream_t st, int64_t* launches) {
+    const int64_t blocks = (kp.ncells + kCellThreads - 1) / kCellThreads;
+    if (blocks > sb.nparts) return cudaErrorInvalidValue;
+    k_cellform<S, T, ESC><<<(unsigned)blocks, kCellThreads, 0, st>>>(
+        (const S*)Vin, (S*)Vout, occ, pol, kp, ctl, sb.part_sum, sb.part_max, argmin);
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cellform(int storage, bool esc, const void* Vin, void* Vout, const uint8_t* occ,
+                            int8_t* pol, const KParams& kp, const float* ctl, const SweepBufs& sb,
+                            int16_t* argmin, cudaStream_t st, int64_t* launches) {
+#define PG_CF(S, T)                                                                            \
+    return esc ? cellform_t<S, T, true>(Vin, Vout, occ, pol, kp, ctl, sb, argmin, st, launches)   \
+               : cellform_t<S, T, false>(Vin, Vout, occ, pol, kp, ctl, sb, argmin, st, launches)
+    switch (storage) {
+        case PG_STORE_F32: PG_CF(float, float);
+        case PG_STORE_F16: PG_CF(__half, float);
+        case PG_STORE_BF16: PG_CF(__nv_bfloat16, float);
+        case PG_STORE_F64: PG_CF(double, double);
+    }
+#undef PG_CF
+    return cudaErrorInvalidValue;
+}
+
+int64_t cellform_blocks(int64_t ncells) { return (ncells + kCellThreads - 1) / kCellThreads; }
+int64_t stencil_blocks(const KParams& kp) { return kp.nplanes * kp.tiles_x; }
+
+size_t stencil_smem(int storage, bool exact, const KParams& kp) {
+    const bool dbl = storage == PG_STORE_F64;
+    if (dbl) return exact ? stencil_smem_bytes<double, true>(kp.nctl, kp.nsub, kp.nchk)
+                          : stencil_smem_bytes<double, false>(kp.nctl, kp.nsub, kp.nchk);
+    return exact ? stencil_smem_bytes<float, true>(kp.nctl, kp.nsub, kp.nchk)
+                 : stencil_smem_bytes<float, false>(kp.nctl, kp.nsub, kp.nchk);
+}
+
+template <typename S, typename T, bool EXACT>
+static cudaError_t stencil_t(const void* Vin, void* Vout, const uint8_t* occ, const KParams& kp,
+                             const float* ctl, const SweepBufs& sb, int16_t* argmin,
+                             cudaStream_t st, int64_t* launches) {
+    const int64_t blocks = stencil_blocks(kp);
+    if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const size_t smem = stencil_smem_bytes<T, EXACT>(kp.nctl, kp.nsub, kp.nchk);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_stencil<S, T, EXACT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_stencil<S, T, EXACT><<<(unsigned)blocks, kStencilThreads, smem, st>>>(
+        (const S*)Vin, (S*)Vout, occ, kp, ctl, sb.part_sum, sb.part_max, argmin);
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout, const uint8_t* occ,
+                           const KParams& kp, const float* ctl, const SweepBufs& sb,
+                           int16_t* argmin, cudaStream_t st, int64_t* launches) {
+#define PG_ST(S, T)                                                                           \
+    return exact ? stencil_t<S, T, true>(Vin, Vout, occ, kp, ctl, sb, argmin, st, launches)     \
+                 : stencil_t<S, T, false>(Vin, Vout, occ, kp, ctl, sb, argmin, st, launches)
+    switch (storage) {
+        case PG_STORE_F32: PG_ST(float, float);
+        case PG_STORE_F16: PG_ST(__half, float);
+        case PG_STORE_BF16: PG_ST(__nv_bfloat16, float);
+        case PG_STORE_F64: PG_ST(double, double);
+    }
+#undef PG_ST
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t dtype,
+                          double scale, double escape_scale, int64_t lo, int64_t n, uint8_t* out,
+                          unsigned long long* counts, cudaStream_t st) {
+    const int b = grid_for(n, 256);
+    switch (storage) {
+        case PG_STORE_F32: k_encode<float><<<b, 256, 0, st>>>((const float*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
+        case PG_STORE_F16: k_encode<__half><<<b, 256, 0, st>>>((const __half*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
+        case PG_STORE_BF16: k_encode<__nv_bfloat16><<<b, 256, 0, st>>>((const __nv_bfloat16*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
+        case PG_STORE_F64: k_encode<double><<<b, 256, 0, st>>>((const double*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pg

@@ -1,0 +1,40 @@
+// pg_kernels.h -- host-side launchers of the sweep, seed, layout and encode
+// kernels (pg_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "pg_types.h"
+
+namespace pg {
+
+cudaError_t launch_fill_seed(int storage, void* V, const KParams& kp, const int64_t* tidx_dev,
+                             int64_t nt, cudaStream_t st);
+cudaError_t launch_seed_only(int storage, void* V, const KParams& kp, const int64_t* tidx_dev,
+                             int64_t nt, cudaStream_t st);
+cudaError_t launch_to_rowmajor(int storage, const void* V, float* out, const KParams& kp,
+                               cudaStream_t st);
+cudaError_t launch_from_rowmajor(int storage, const float* in, void* V, const KParams& kp,
+                                 cudaStream_t st);
+cudaError_t launch_convert_to_f32(int storage, const void* in, float* out, int64_t n,
+                                  cudaStream_t st);
+cudaError_t launch_cellform(int storage, bool esc, const void* Vin, void* Vout,
+                            const uint8_t* occ, int8_t* pol, const KParams& kp, const float* ctl,
+                            const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                            int64_t* launches);
+cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout,
+                           const uint8_t* occ, const KParams& kp, const float* ctl,
+                           const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                           int64_t* launches);
+cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t dtype,
+                          double scale, double escape_scale, int64_t lo, int64_t n, uint8_t* out,
+                          unsigned long long* counts, cudaStream_t st);
+
+int64_t cellform_blocks(int64_t ncells);
+int64_t stencil_blocks(const KParams& kp);
+size_t stencil_smem(int storage, bool exact, const KParams& kp);
+
+}  // namespace pg

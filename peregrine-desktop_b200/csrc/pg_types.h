@@ -1,0 +1,42 @@
+// pg_types.h -- internal types shared by the kernels and the C-ABI layer.
+#pragma once
+
+#include <cstdint>
+
+#include "peregrine_hjb.h"
+
+namespace pg {
+
+// Largest substep count / probe count the stencil kernel stages in shared
+// memory.  Schemes beyond these run on the cell-form kernel.
+constexpr int kStencilMaxSub = 16;
+constexpr int kStencilMaxChk = 24;
+constexpr int kStencilThreads = 256;
+constexpr int kCellThreads = 128;
+
+// Everything a sweep kernel needs besides the arrays, passed by value.
+struct KParams {
+    pg_grid6 g;
+    pg_model m;
+    pg_params p;
+    int64_t P;        // Nx*Ny, one (h, v) plane
+    int64_t nplanes;  // Nh*Nvx*Nvy*Nw
+    int64_t ncells;
+    int32_t nctl;
+    int32_t tile_x;   // stencil: x rows per block
+    int32_t tiles_x;  // stencil: blocks per plane
+    int32_t nsub;     // stencil: substeps of the single horizon
+    int32_t nchk;     // stencil: swept probes per lookahead
+    int32_t phase;
+};
+
+// Per-sweep reduction buffers: one partial per block, reduced in a fixed
+// order so the convergence signal is bit-for-bit reproducible.
+struct SweepBufs {
+    double* part_sum;
+    double* part_max;
+    int64_t nparts;
+    double* out;  // [2]: L1 total, max-norm
+};
+
+}  // namespace pg

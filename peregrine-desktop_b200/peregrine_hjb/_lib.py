@@ -1,0 +1,286 @@
+"""ctypes binding of libperegrine_hjb.so (include/peregrine_hjb.h).
+
+The library is the only compute path: there is no CPU fallback.  Loading
+fails loudly when the shared object is missing, and every call that returns a
+negative status raises :class:`PeregrineError` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_NAME = "libperegrine_hjb.so"
+LIB_PATH = Path(__file__).resolve().parent / LIB_NAME
+
+PG_OK = 0
+PG_EINVAL, PG_ECUDA, PG_ENOMEM, PG_ETIMEOUT, PG_ESTATE, PG_EUNSUPPORTED, PG_ECANCELLED = (
+    -1, -2, -3, -4, -5, -6, -7)
+
+STOP_L1_QUIET, STOP_MAXNORM = 0, 1
+STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
+STORAGES = {"fp32": STORE_F32, "fp16": STORE_F16, "bf16": STORE_BF16, "fp64": STORE_F64}
+KERNEL_AUTO, KERNEL_STENCIL, KERNEL_CELLFORM, KERNEL_STENCIL_EXACT = 0, 1, 2, 3
+DTYPE_CODES = {"u8": 0, "u16": 1, "f16": 2, "f32": 3}
+
+# Every symbol include/peregrine_hjb.h declares.
+EXPORTS = (
+    "pg_abi_version", "pg_last_error", "pg_default_opts", "pg_create", "pg_destroy",
+    "pg_solve_value", "pg_load_problem", "pg_solve", "pg_get_value", "pg_set_value",
+    "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
+    "pg_launch_count",
+)
+
+
+class PeregrineError(RuntimeError):
+    """A negative status from the library, with its message."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+class Grid6(C.Structure):
+    _fields_ = [("n", C.c_int32 * 6), ("lo", C.c_float * 6), ("step", C.c_float * 6)]
+
+
+class Model(C.Structure):
+    _fields_ = [("B", C.c_float * 9), ("A", C.c_float * 9), ("q", C.c_float * 3),
+                ("S", C.c_float * 9), ("D", C.c_float * 9), ("c", C.c_float * 3),
+                ("eps", C.c_float * 3), ("knee", C.c_float)]
+
+
+class Params(C.Structure):
+    _fields_ = [("dt", C.c_float), ("nsub", C.c_int32), ("checks", C.c_int32),
+                ("adaptive_checks", C.c_int32), ("nearest", C.c_int32), ("cap", C.c_float),
+                ("ntau", C.c_int32), ("tau_ratio", C.c_float), ("cfl", C.c_float),
+                ("tau_min", C.c_float), ("tau_max", C.c_float), ("hmax", C.c_float),
+                ("ncoarse", C.c_int32), ("rounds", C.c_int32), ("delta0", C.c_float),
+                ("rk2", C.c_int32), ("vclamp", C.c_int32), ("simplex", C.c_int32)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("stop_rule", C.c_int32), ("storage", C.c_int32), ("kernel", C.c_int32),
+                ("warm_start", C.c_int32), ("polish_sweeps", C.c_int32),
+                ("progress_every", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
+class SolveResult(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("polish_iterations", C.c_int32),
+                ("last_delta", C.c_double), ("last_maxnorm", C.c_double),
+                ("kernel_ms", C.c_double), ("elapsed_ms", C.c_double),
+                ("cell_controls", C.c_int64)]
+
+
+PROGRESS_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_double, C.c_double)
+
+_lib = None
+
+
+def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load libperegrine_hjb.so once; raise if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"{p} is missing: build the CUDA library first "
+            "(make -C peregrine-desktop_b200/csrc, or __graft_entry__.build()). "
+            "There is no CPU fallback.")
+    lib = C.CDLL(str(p))
+    vp, i32, i64, f64 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    P = C.POINTER
+    sig = {
+        "pg_abi_version": (i32, []),
+        "pg_last_error": (C.c_char_p, []),
+        "pg_default_opts": (None, [P(SolveOpts)]),
+        "pg_create": (C.c_int, [P(vp), C.c_int]),
+        "pg_destroy": (C.c_int, [vp]),
+        "pg_solve_value": (C.c_int, [vp, P(Grid6), P(Model), P(Params), vp, vp, i64, vp, i32,
+                                     i32, f64, P(SolveOpts), vp, P(SolveResult), PROGRESS_CB, vp]),
+        "pg_load_problem": (C.c_int, [vp, P(Grid6), P(Model), P(Params), vp, vp, i32, i32]),
+        "pg_solve": (C.c_int, [vp, vp, i64, i32, f64, P(SolveOpts), P(SolveResult),
+                               PROGRESS_CB, vp]),
+        "pg_get_value": (C.c_int, [vp, vp]),
+        "pg_set_value": (C.c_int, [vp, vp]),
+        "pg_sweep": (C.c_int, [vp, i32, i32, P(f64), P(f64), vp]),
+        "pg_escape_sweep": (C.c_int, [vp, i32, P(f64)]),
+        "pg_solve_escape": (C.c_int, [vp, i32, f64, P(SolveResult), PROGRESS_CB, vp]),
+        "pg_encode": (C.c_int, [vp, i32, f64, f64, i64, i64, vp, P(i64), P(i64)]),
+        "pg_time_sweeps": (C.c_int, [vp, i32, i32, i32, P(f64)]),
+        "pg_launch_count": (C.c_int, [vp, P(i64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.pg_abi_version() != 1:
+        raise RuntimeError(f"{p}: unexpected ABI version {lib.pg_abi_version()}")
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != PG_OK:
+        msg = _lib.pg_last_error().decode("utf-8", "replace") if _lib else "library not loaded"
+        raise PeregrineError(rc, msg)
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def default_opts(**kw) -> SolveOpts:
+    lib = load_library()
+    o = SolveOpts()
+    lib.pg_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if k == "storage" and isinstance(v, str):
+            v = STORAGES[v]
+        setattr(o, k, int(v))
+    return o
+
+
+class Context:
+    """One device context: a stream plus the buffers of one loaded problem."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        h = C.c_void_p()
+        _check(self._lib.pg_create(C.byref(h), int(device)))
+        self._h = h
+        self.ncells = 0
+        self.nctl = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.pg_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_problem(self, grid: Grid6, model: Model, params: Params, occ: np.ndarray,
+                     ctl: np.ndarray, storage: int | str = STORE_F32) -> None:
+        if isinstance(storage, str):
+            storage = STORAGES[storage]
+        occ = np.ascontiguousarray(occ, dtype=np.uint8)
+        ctl = np.ascontiguousarray(ctl, dtype=np.float32)
+        nctl = ctl.size // 3
+        n = [int(v) for v in grid.n]
+        if occ.size != n[0] * n[1] * n[2]:
+            raise ValueError(f"occupancy has {occ.size} entries, expected {n[0] * n[1] * n[2]}")
+        _check(self._lib.pg_load_problem(self._h, C.byref(grid), C.byref(model),
+                                         C.byref(params), _ptr(occ), _ptr(ctl), nctl,
+                                         int(storage)))
+        self.ncells = int(np.prod(np.array(n, dtype=np.int64)))
+        self.nctl = nctl
+        self._keep = (occ, ctl)
+
+    def solve(self, tidx: np.ndarray, iters: int, tol: float, opts: SolveOpts | None = None,
+              progress=None) -> SolveResult:
+        tidx = np.ascontiguousarray(tidx, dtype=np.int64)
+        res = SolveResult()
+        cb = _wrap_cb(progress)
+        _check(self._lib.pg_solve(self._h, _ptr(tidx), tidx.size, int(iters), float(tol),
+                                  C.byref(opts) if opts is not None else None, C.byref(res),
+                                  cb, None))
+        return res
+
+    def solve_escape(self, iters: int, tol: float, progress=None) -> SolveResult:
+        res = SolveResult()
+        _check(self._lib.pg_solve_escape(self._h, int(iters), float(tol), C.byref(res),
+                                         _wrap_cb(progress), None))
+        return res
+
+    def get_value(self) -> np.ndarray:
+        out = np.empty(self.ncells, dtype=np.float32)
+        _check(self._lib.pg_get_value(self._h, _ptr(out)))
+        return out
+
+    def set_value(self, V: np.ndarray) -> None:
+        V = np.ascontiguousarray(V, dtype=np.float32)
+        if V.size != self.ncells:
+            raise ValueError("value array has the wrong size")
+        _check(self._lib.pg_set_value(self._h, _ptr(V)))
+
+    def sweep(self, phase: int = 0, kernel: int = KERNEL_AUTO, argmin: bool = False):
+        d = C.c_double()
+        dm = C.c_double()
+        am = np.empty(self.ncells, dtype=np.int16) if argmin else None
+        _check(self._lib.pg_sweep(self._h, int(phase), int(kernel), C.byref(d), C.byref(dm),
+                                  _ptr(am)))
+        return d.value, dm.value, am
+
+    def escape_sweep(self, phase: int = 0) -> float:
+        d = C.c_double()
+        _check(self._lib.pg_escape_sweep(self._h, int(phase), C.byref(d)))
+        return d.value
+
+    def encode(self, dtype: str, scale: float, escape_scale: float, lo: int, n: int,
+               out: np.ndarray | None = None):
+        eb = {"u8": 1, "u16": 2, "f16": 2, "f32": 4}[dtype]
+        if out is None:
+            out = np.empty(n * eb, dtype=np.uint8)
+        r = C.c_int64()
+        e = C.c_int64()
+        _check(self._lib.pg_encode(self._h, DTYPE_CODES[dtype], float(scale), float(escape_scale),
+                                   int(lo), int(n), _ptr(out), C.byref(r), C.byref(e)))
+        return out[: n * eb], r.value, e.value
+
+    def time_sweeps(self, warmup: int, steps: int, kernel: int = KERNEL_AUTO) -> float:
+        ms = C.c_double()
+        _check(self._lib.pg_time_sweeps(self._h, int(warmup), int(steps), int(kernel),
+                                        C.byref(ms)))
+        return ms.value
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        _check(self._lib.pg_launch_count(self._h, C.byref(n)))
+        return n.value
+
+
+def _wrap_cb(progress):
+    if progress is None:
+        return PROGRESS_CB()
+
+    def _cb(_user, it, d, dm):
+        try:
+            return 1 if progress(int(it), float(d), float(dm)) else 0
+        except Exception:  # never let a Python exception unwind through C
+            return 1
+
+    return PROGRESS_CB(_cb)
+
+
+def solve_value(grid: Grid6, model: Model, params: Params, occ: np.ndarray, tidx: np.ndarray,
+                ctl: np.ndarray, iters: int, tol: float, opts: SolveOpts | None = None,
+                device: int = 0, progress=None):
+    """One-shot mirror of solve_value! (Run.jl:1434-1474): host buffers in,
+    host V (row-major float32) and the result record out."""
+    lib = load_library()
+    with Context(device) as ctx:
+        occ = np.ascontiguousarray(occ, dtype=np.uint8)
+        ctl = np.ascontiguousarray(ctl, dtype=np.float32)
+        tidx = np.ascontiguousarray(tidx, dtype=np.int64)
+        n = int(np.prod(np.array([int(v) for v in grid.n], dtype=np.int64)))
+        V = np.empty(n, dtype=np.float32)
+        res = SolveResult()
+        _check(lib.pg_solve_value(ctx._h, C.byref(grid), C.byref(model), C.byref(params),
+                                  _ptr(occ), _ptr(tidx), tidx.size, _ptr(ctl), ctl.size // 3,
+                                  int(iters), float(tol),
+                                  C.byref(opts) if opts is not None else None, _ptr(V),
+                                  C.byref(res), _wrap_cb(progress), None))
+        return V, res

@@ -1,0 +1,279 @@
+"""The CUDA path against the CPU oracle, through the C ABI.
+
+Bit-exact where the kernel keeps the reference's operation order (the
+cell-form kernel and the exact stencil instantiation); within a stated
+tolerance where it does not (the FMA stencil: 2e-5 s per sweep, 1e-4 s at
+the fixed point, argmin agreement >= 99.9%).
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+from peregrine_hjb import _lib
+from peregrine_hjb.synth import Problem
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+
+FMA_SWEEP_TOL = 2e-5     # s, one sweep, FMA stencil vs oracle
+FIXED_POINT_TOL = 1e-4   # s, converged tables, FMA stencil vs oracle
+ARGMIN_AGREE = 0.999
+
+
+def oracle_structs(og, pr):
+    g = og.copy_struct(pr.grid.to_c(), og.OGrid)
+    m = og.copy_struct(pr.model.to_c(), og.OModel)
+    p = og.copy_struct(pr.params, og.OParams)
+    return g, m, p
+
+
+def init_value(pr):
+    V = np.full(pr.ncells, np.float32(pr.params.cap), np.float32)
+    V[pr.seeds] = 0.0
+    return V
+
+
+@pytest.fixture(scope="module")
+def tiny():
+    return Problem("tiny", seed=5)
+
+
+@pytest.fixture(scope="module")
+def tiny_state(og, tiny):
+    """A structured V: the initial table after four oracle sweeps."""
+    g, m, p = oracle_structs(og, tiny)
+    V = init_value(tiny)
+    for it in range(4):
+        V, _, _, _ = og.sweep_jacobi(V, tiny.occ, g, m, tiny.ctl, p, phase=it)
+        V[tiny.seeds] = 0.0
+    return V
+
+
+def gpu_ctx(pr, storage="fp32", params=None):
+    ctx = _lib.Context(0)
+    ctx.load_problem(pr.grid.to_c(), pr.model.to_c(), params or pr.params, pr.occ, pr.ctl, storage)
+    return ctx
+
+
+@pytest.mark.parametrize("kernel", [_lib.KERNEL_CELLFORM, _lib.KERNEL_STENCIL_EXACT])
+def test_one_sweep_bit_exact(og, tiny, tiny_state, kernel):
+    g, m, p = oracle_structs(og, tiny)
+    want, tot, mx, am = og.sweep_jacobi(tiny_state, tiny.occ, g, m, tiny.ctl, p, phase=4, argmin=True)
+    with gpu_ctx(tiny) as ctx:
+        ctx.set_value(tiny_state)
+        d, dm, gam = ctx.sweep(phase=4, kernel=kernel, argmin=True)
+        got = ctx.get_value()
+    assert np.array_equal(got, want), f"max |dV| {np.max(np.abs(got - want))}"
+    assert np.array_equal(gam, am)
+    assert mx == dm
+    assert abs(d - tot) <= 1e-9 * max(1.0, tot)
+
+
+def test_one_sweep_fma_stencil_within_tolerance(og, tiny, tiny_state):
+    g, m, p = oracle_structs(og, tiny)
+    want, tot, mx, am = og.sweep_jacobi(tiny_state, tiny.occ, g, m, tiny.ctl, p, phase=4, argmin=True)
+    with gpu_ctx(tiny) as ctx:
+        ctx.set_value(tiny_state)
+        _, _, gam = ctx.sweep(phase=4, kernel=_lib.KERNEL_STENCIL, argmin=True)
+        got = ctx.get_value()
+    assert np.max(np.abs(got - want)) <= FMA_SWEEP_TOL
+    free = am >= 0
+    assert np.mean(gam[free] == am[free]) >= ARGMIN_AGREE
+
+
+def test_one_sweep_small_slab_bit_exact(og):
+    """The 24x24x16x9x9x9 workload (27 controls), one x-slab against the oracle."""
+    pr = Problem("small", seed=0)
+    g, m, p = oracle_structs(og, pr)
+    V0 = init_value(pr)
+    with gpu_ctx(pr) as ctx:
+        ctx.set_value(V0)
+        for it in range(6):
+            ctx.sweep(phase=it, kernel=_lib.KERNEL_STENCIL_EXACT)
+        Vk = ctx.get_value()
+        slab = pr.ncells // pr.grid.n[0]
+        lo, hi = 11 * slab, 13 * slab
+        want, _, _, am = og.sweep_jacobi(Vk, pr.occ, g, m, pr.ctl, p, phase=6, lo=lo, hi=hi,
+                                         argmin=True)
+        ctx.set_value(Vk)
+        _, _, gam = ctx.sweep(phase=6, kernel=_lib.KERNEL_STENCIL_EXACT, argmin=True)
+        got = ctx.get_value()
+    assert np.array_equal(got[lo:hi], want[lo:hi])
+    assert np.array_equal(gam[lo:hi], am[lo:hi])
+
+
+def test_fixed_point_matches_oracle(og, tiny):
+    """Converged tables (max-norm stop at 1e-4 s): FMA stencil vs the oracle's
+    Jacobi solve on the same inputs."""
+    g, m, p = oracle_structs(og, tiny)
+    Vo, it_o, _, _ = og.solve_value(tiny.occ, g, m, tiny.seeds, tiny.ctl, p, 3000, 1e-4,
+                                    stop_rule=1, jacobi=True)
+    opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL)
+    V, res = _lib.solve_value(tiny.grid.to_c(), tiny.model.to_c(), tiny.params, tiny.occ,
+                              tiny.seeds, tiny.ctl, 3000, 1e-4, opts)
+    assert abs(res.iterations - it_o) <= 2
+    err = np.abs(V - Vo)
+    assert err.max() <= FIXED_POINT_TOL, f"max {err.max()} rms {np.sqrt(np.mean(err ** 2))}"
+    _, _, _, am_o = og.sweep_jacobi(Vo, tiny.occ, g, m, tiny.ctl, p, argmin=True)
+    with gpu_ctx(tiny) as ctx:
+        ctx.set_value(V)
+        _, _, am_g = ctx.sweep(kernel=_lib.KERNEL_STENCIL, argmin=True)
+    free = am_o >= 0
+    assert np.mean(am_g[free] == am_o[free]) >= ARGMIN_AGREE
+
+
+def test_cellform_solve_bit_exact_with_reference_defaults(og, tiny):
+    """The reference's default scheme (warm start, rotating scan, pattern
+    search, CFL ladder, adaptive probes, Kuhn simplex) on the cell-form
+    kernel: three sweeps bit-identical to the oracle's."""
+    pr = tiny
+    p = _lib.Params()
+    C.memmove(C.byref(p), C.byref(pr.params), C.sizeof(p))
+    p.ncoarse, p.rounds, p.ntau, p.cfl, p.adaptive_checks, p.simplex = 8, 2, 5, 2.0, 1, 1
+    p.tau_max, p.hmax = 0.5, 0.0125
+    g, m, _ = oracle_structs(og, pr)
+    po = og.copy_struct(p, og.OParams)
+    Vo, _, _, _ = og.solve_value(pr.occ, g, m, pr.seeds, pr.ctl, po, 3, 0.0, jacobi=True, warm=True)
+    opts = _lib.default_opts(kernel=_lib.KERNEL_CELLFORM, warm_start=1)
+    V, res = _lib.solve_value(pr.grid.to_c(), pr.model.to_c(), p, pr.occ, pr.seeds, pr.ctl, 3,
+                              0.0, opts)
+    assert res.iterations == 3
+    assert np.array_equal(V, Vo), f"max |dV| {np.max(np.abs(V - Vo))}"
+
+
+def test_escape_sweeps_bit_exact(og, tiny, tiny_state):
+    g, m, p = oracle_structs(og, tiny)
+    Vo = tiny_state.copy()
+    with gpu_ctx(tiny) as ctx:
+        ctx.set_value(tiny_state)
+        for it in range(3):
+            Vo, tot = og.sweep_escape_jacobi(Vo, tiny.occ, g, m, tiny.ctl, p, phase=it)
+            d = ctx.escape_sweep(phase=it)
+            assert abs(d - tot) <= 1e-9 * max(1.0, tot)
+        got = ctx.get_value()
+    assert np.array_equal(got, Vo)
+    assert np.any(Vo < 0)
+
+
+@pytest.mark.parametrize("dtype", ["u16", "u8", "f16", "f32"])
+def test_encode_byte_identical(og, tiny, dtype):
+    from peregrine_hjb.tables import DTYPES, escape_scale_for
+    cap = float(tiny.params.cap)
+    rng = np.random.default_rng(9)
+    n = tiny.ncells
+    V = rng.uniform(0, cap, n).astype(np.float32)
+    k = rng.integers(0, 7, n)
+    V[k == 0] = cap
+    V[k == 1] = -rng.uniform(0, cap, np.sum(k == 1)).astype(np.float32)
+    V[k == 2] = np.round(V[k == 2] * 1000) / 1000 + 0.0005  # rounding ties in the codes
+    V[:4] = [np.inf, np.nan, -0.0, 0.0]
+    es = escape_scale_for(dtype, cap)
+    sc = DTYPES[dtype]["scale"]
+    want, r, e = og.encode(V, dtype, sc, cap, es)
+    with gpu_ctx(tiny) as ctx:
+        ctx.set_value(V)
+        got, gr, ge = ctx.encode(dtype, sc, es, 0, n)
+        lo = 1000
+        part, _, _ = ctx.encode(dtype, sc, es, lo, 5000)
+    assert bytes(got) == bytes(want)
+    assert (gr, ge) == (r, e)
+    eb = DTYPES[dtype]["bytes"]
+    assert bytes(part) == bytes(want[lo * eb:(lo + 5000) * eb])
+
+
+def test_fp64_and_16bit_storage(og, tiny):
+    """FP64 device oracle vs FP32, and FP16/BF16 storage with FP32 polish vs
+    FP32, on converged tables (max-norm stop 1e-4 s)."""
+    args = (tiny.grid.to_c(), tiny.model.to_c(), tiny.params, tiny.occ, tiny.seeds, tiny.ctl,
+            3000, 1e-4)
+    V32, _ = _lib.solve_value(*args, _lib.default_opts(stop_rule=1))
+    V64, _ = _lib.solve_value(*args, _lib.default_opts(stop_rule=1, storage="fp64"))
+    V16, r16 = _lib.solve_value(*args, _lib.default_opts(stop_rule=1, storage="fp16",
+                                                         polish_sweeps=400))
+    Vbf, rbf = _lib.solve_value(*args, _lib.default_opts(stop_rule=1, storage="bf16",
+                                                         polish_sweeps=800))
+    assert np.max(np.abs(V64 - V32)) < 5e-3
+    assert np.max(np.abs(V16 - V32)) <= 2e-3
+    assert np.max(np.abs(Vbf - V32)) <= 2e-3
+    assert r16.polish_iterations >= 1
+
+
+def test_minimum_time_closed_form():
+    """SelfTest [1] (SelfTest.jl:90-199): the bang-bang minimum time 2*sqrt(d/a)
+    of a double integrator, with the reference's three schemes on its grid."""
+    from peregrine_hjb.grid import Grid6
+    from peregrine_hjb.params import control_set
+    from peregrine_hjb.seeds import target_cells
+    g = Grid6.make((81, 5, 4, 33, 5, 5), (0, 0, -math.pi, -100, -100, -2), (200, 200, math.pi, 100, 100, 2))
+    amax = 100.0
+    m = _lib.Model()
+    for i, v in enumerate((amax, 0, 0, 0, amax, 0, 0, 0, amax)):
+        m.B[i] = v
+    m.eps[0], m.eps[1], m.eps[2] = 5.0, 5.0, 0.15
+    m.knee = 0.0
+    occ = np.zeros(81 * 5 * 4, np.uint8)
+    ttol = tuple(np.float32(g.step[k] * np.float32(0.5)) for k in range(6))
+    tc = target_cells(g, (np.float32(100), np.float32(100), 0, 0, 0, 0), ttol)
+    ctl = control_set(4)
+
+    def params(**kw):
+        p = _lib.Params()
+        base = dict(dt=0.05, nsub=4, checks=3, adaptive_checks=1, nearest=0, cap=30.0, ntau=1,
+                    tau_ratio=2.0, cfl=0.0, tau_min=0.004, tau_max=0.5, hmax=0.0125, ncoarse=0,
+                    rounds=0, delta0=0.35, rk2=1, vclamp=0, simplex=1)
+        base.update(kw)
+        for k, v in base.items():
+            setattr(p, k, v)
+        return p
+
+    def run(p, warm):
+        opts = _lib.default_opts(kernel=_lib.KERNEL_CELLFORM, warm_start=int(warm))
+        V, _ = _lib.solve_value(g.to_c(), m, p, occ, tc, ctl, 600, 1e-4, opts)
+        return V
+
+    legacy = run(params(checks=3, adaptive_checks=0, ntau=1, cfl=0.0, ncoarse=0, rounds=0, rk2=0), False)
+    ladder = run(params(checks=2, adaptive_checks=1, ntau=4, cfl=1.0, ncoarse=0, rounds=0, rk2=1), False)
+    now = run(params(checks=2, adaptive_checks=1, ntau=4, cfl=1.0, ncoarse=8, rounds=2, rk2=1), True)
+    from oracle import oracle as og
+    og_g = og.copy_struct(g.to_c(), og.OGrid)
+    ds = (20.0, 40.0, 60.0)
+    want = [2.0 * math.sqrt(d / amax) for d in ds]
+
+    def at(V, d):
+        return float(og.lib().og_interp_kuhn(V.ctypes.data, og_g, og.state(100.0 - d, 100.0, 0, 0, 0, 0),
+                                             30.0, 0, None))
+
+    gotl = [at(legacy, d) for d in ds]
+    gotd = [at(ladder, d) for d in ds]
+    gotn = [at(now, d) for d in ds]
+    ml, md, mn = sum(gotl) / 3, sum(gotd) / 3, sum(gotn) / 3
+    assert mn <= md * 1.08
+    assert md <= ml * 1.02
+    ex = [gotn[i] - want[i] for i in range(3)]
+    slope = (ex[2] - ex[0]) / (want[2] - want[0])
+    intercept = ex[0] - slope * want[0]
+    assert intercept < 0.45 and slope < 0.20
+
+
+def test_full_size_properties():
+    """The 48x48x32x15x15x15 workload (125 controls): size-independent
+    properties of a few sweeps -- monotone, bounded, seeds pinned, the
+    residual equals the largest change."""
+    pr = Problem("medium", seed=0)
+    cap = np.float32(pr.params.cap)
+    with gpu_ctx(pr) as ctx:
+        opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM)
+        res = ctx.solve(pr.seeds, 3, 0.0, opts)
+        V1 = ctx.get_value()
+        d, dm, _ = ctx.sweep(phase=3)
+        V2 = ctx.get_value()
+    assert res.iterations == 3
+    assert np.all(V2 <= V1) and np.all(V2 >= 0) and np.all(V2 <= cap)
+    assert np.all(V2[pr.seeds] == 0)
+    diff = V1.astype(np.float64) - V2.astype(np.float64)
+    assert float(np.max(diff)) == dm
+    assert abs(float(np.sum(diff)) - d) <= 1e-9 * max(1.0, d)
+    assert np.count_nonzero(V2 < cap) > np.count_nonzero(V1 < cap) or dm == 0
