@@ -226,6 +226,14 @@ def run_ours(args, rank, world, local_rank):
     ms_max = float(t.item())
     cc_per_sweep = pr.ncells * pr.nctl
     value = world * cc_per_sweep / (ms_max / 1000.0)
+    if args.only_device:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                              "workload": WORKLOAD, "gpu_launches": launches,
+                              "clocks": clk.summary(), "only_device": True}), flush=True)
+        ctx.close()
+        return 0
 
     # ---- end to end through the public one-shot call, host buffers in/out
     e2e_sweeps = 2
@@ -307,7 +315,14 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD,
+                    help="synthetic workload (medium is the benchmark; medium_h8 is the "
+                         "same planes and controls with 8 headings, for profiler captures)")
+    ap.add_argument("--only-device", action="store_true",
+                    help="time the device sweeps only (no end-to-end leg, no CPU baseline); "
+                         "for profiler captures")
     args = ap.parse_args()
+    globals()["WORKLOAD"] = args.workload
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "pg_kernels.h"
@@ -75,6 +76,8 @@ struct pg_ctx {
     int cur = 0;
     uint8_t* occ_d = nullptr;
     float* ctl_d = nullptr;
+    int32_t* order_d = nullptr;
+    std::vector<int32_t> order_h;
     int8_t* pol_d = nullptr;
     double* part_sum = nullptr;
     double* part_max = nullptr;
@@ -101,6 +104,8 @@ struct pg_ctx {
         free_values();
         if (occ_d) cudaFree(occ_d);
         if (ctl_d) cudaFree(ctl_d);
+        if (order_d) cudaFree(order_d);
+        order_d = nullptr;
         if (pol_d) cudaFree(pol_d);
         if (part_sum) cudaFree(part_sum);
         if (part_max) cudaFree(part_max);
@@ -180,8 +185,8 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
                                 ctx->stream, &ctx->launches);
     else
         e = pg::launch_stencil(ctx->storage, kernel == PG_KERNEL_STENCIL_EXACT, vin, vout,
-                               ctx->occ_d, ctx->kp, ctx->ctl_d, sb, argmin_d, ctx->stream,
-                               &ctx->launches);
+                               ctx->occ_d, ctx->kp, ctx->ctl_d, ctx->order_d, sb, argmin_d,
+                               ctx->stream, &ctx->launches);
     if (e != cudaSuccess) return fail(PG_ECUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
     ctx->cur = 1 - ctx->cur;
     return PG_OK;
@@ -337,12 +342,29 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     kp.nplanes = (int64_t)g->n[2] * g->n[3] * g->n[4] * g->n[5];
     kp.ncells = kp.P * kp.nplanes;
     kp.nctl = nctl;
-    // x rows per stencil block: about 2048 cells, never more than the plane
-    int32_t tx = (int32_t)((2048 + g->n[1] - 1) / g->n[1]);
-    if (tx < 1) tx = 1;
-    if (tx > g->n[0]) tx = g->n[0];
-    kp.tile_x = tx;
-    kp.tiles_x = (g->n[0] + tx - 1) / tx;
+    // Stencil tiling: a block takes whole planes (x rows split only past 4096
+    // four-cell segments), and the block size is the multiple of 32 in
+    // [96, 256] that leaves the fewest idle threads in the last pass.
+    {
+        const int32_t spr = (g->n[1] + 3) / 4;
+        const int64_t segs_plane = (int64_t)g->n[0] * spr;
+        const int64_t ntile = (segs_plane + 4095) / 4096;
+        int32_t tx = (int32_t)((g->n[0] + ntile - 1) / ntile);
+        kp.tile_x = tx;
+        kp.tiles_x = (g->n[0] + tx - 1) / tx;
+        const int64_t segs = (int64_t)tx * spr;
+        int best_bs = 256;
+        int64_t best_waste = -1;
+        if (segs < 96) {
+            best_bs = (int)(32 * ((segs + 31) / 32));
+        } else {
+            for (int bs = 256; bs >= 96; bs -= 32) {
+                const int64_t waste = ((segs + bs - 1) / bs) * bs - segs;
+                if (best_waste < 0 || waste < best_waste) { best_waste = waste; best_bs = bs; }
+            }
+        }
+        kp.block = best_bs;
+    }
     kp.nsub = host_substeps_for(p->cfl <= 0.0f ? p->dt : p->tau_max, *p);
     kp.nchk = p->checks;
 
@@ -361,7 +383,7 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     if (p->nearest) no("nearest");
     if (p->simplex) no("simplex (Kuhn) interpolation");
     if (kp.nsub > pg::kStencilMaxSub) no("more than 16 substeps");
-    if (p->checks > pg::kStencilMaxChk) no("more than 24 probes");
+    if (p->checks > pg::kStencilMaxChk) no("more than 4 swept probes");
     if (kp.ncells / kp.tiles_x > (int64_t)1 << 40) no("grid too large");
 
     ctx->ctl_h.assign(ctl, ctl + 3 * nctl);
@@ -381,6 +403,21 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     PG_CUDA(cudaMalloc(&ctx->ctl_d, sizeof(float) * 3 * nctl));
     PG_CUDA(cudaMemcpyAsync(ctx->ctl_d, ctl, sizeof(float) * 3 * nctl, cudaMemcpyHostToDevice,
                             ctx->stream));
+    // The stencil visits controls in (u1, u2, u3) order, so consecutive
+    // controls land on neighbouring successor planes and reuse them from L1;
+    // its tie-break on the table index keeps the result order-independent.
+    ctx->order_h.resize(nctl);
+    for (int32_t k = 0; k < nctl; ++k) ctx->order_h[k] = k;
+    std::stable_sort(ctx->order_h.begin(), ctx->order_h.end(), [&](int32_t a, int32_t b) {
+        for (int c = 0; c < 3; ++c) {
+            const float ua = ctl[a + c * nctl], ub = ctl[b + c * nctl];
+            if (ua != ub) return ua < ub;
+        }
+        return a < b;
+    });
+    PG_CUDA(cudaMalloc(&ctx->order_d, sizeof(int32_t) * nctl));
+    PG_CUDA(cudaMemcpyAsync(ctx->order_d, ctx->order_h.data(), sizeof(int32_t) * nctl,
+                            cudaMemcpyHostToDevice, ctx->stream));
     ctx->nparts = pg::cellform_blocks(kp.ncells);
     const int64_t sb = pg::stencil_blocks(kp);
     if (sb > ctx->nparts) ctx->nparts = sb;

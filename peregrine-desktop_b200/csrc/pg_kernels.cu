@@ -33,11 +33,16 @@
 
 namespace pg {
 
+// 16-bit storage rounds UP.  Value iteration here only ever lowers a cell,
+// so a stored value must stay an upper bound of the FP32 iterate: a value
+// rounded to nearest can land below the fixed point, and no later sweep (16-
+// or 32-bit) can raise it again.  Rounded up, the 16-bit phase stops at or
+// above the FP32 fixed point and the FP32 polish sweeps descend onto it.
 template <> struct Conv<__half> {
     static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
     static __device__ __forceinline__ float val(__half v) { return __half2float(v); }
     template <typename T> static __device__ __forceinline__ __half st(T v) {
-        return __float2half_rn((float)v);
+        return __float2half_ru((float)v);
     }
 };
 template <> struct Conv<__nv_bfloat16> {
@@ -46,7 +51,7 @@ template <> struct Conv<__nv_bfloat16> {
     }
     static __device__ __forceinline__ float val(__nv_bfloat16 v) { return __bfloat162float(v); }
     template <typename T> static __device__ __forceinline__ __nv_bfloat16 st(T v) {
-        return __float2bfloat16_rn((float)v);
+        return __float2bfloat16_ru((float)v);
     }
 };
 
@@ -545,275 +550,7 @@ __global__ void __launch_bounds__(kCellThreads)
     block_partial(dsum, dmax, part_sum, part_max);
 }
 
-// ---------------------------------------------------------------------------
-// The plain scheme as a position-invariant stencil
-// ---------------------------------------------------------------------------
-
-// Shared-memory staging of one plane's transitions, structure of arrays
-// indexed [item][control] so a warp reading one control broadcasts.
-template <typename T> struct StencilSmem {
-    T* incx;       // [nsub][nctl]
-    T* incy;       // [nsub][nctl]
-    T* w;          // EXACT: [8][nctl] (1-t, t for h, vx, vy, w); fast: [16][nctl] products
-    T* aprobe;     // [nchk]
-    int32_t* plane;// [16][nctl] corner plane indices
-    int32_t* ck;   // [nchk][nctl] probe heading bins
-    int32_t* ok;   // [nctl]
-    T* tau;        // [nctl]
-};
-
-template <typename T, bool EXACT>
-__host__ __device__ inline size_t stencil_smem_bytes(int nctl, int nsub, int nchk) {
-    size_t nt = (size_t)(2 * nsub + (EXACT ? 8 : 16) + 1) * nctl + nchk;
-    size_t ni = (size_t)(16 + nchk + 1) * nctl;
-    return nt * sizeof(T) + ni * sizeof(int32_t) + 64;
-}
-
-template <typename T, bool EXACT>
-__device__ __forceinline__ StencilSmem<T> carve(unsigned char* base, int nctl, int nsub, int nchk) {
-    StencilSmem<T> s;
-    T* tp = (T*)base;
-    s.incx = tp; tp += (size_t)nsub * nctl;
-    s.incy = tp; tp += (size_t)nsub * nctl;
-    s.w = tp; tp += (size_t)(EXACT ? 8 : 16) * nctl;
-    s.tau = tp; tp += nctl;
-    s.aprobe = tp; tp += nchk;
-    int32_t* ip = (int32_t*)tp;
-    s.plane = ip; ip += 16 * nctl;
-    s.ck = ip; ip += (size_t)nchk * nctl;
-    s.ok = ip;
-    return s;
-}
-
-template <typename S, typename T, bool EXACT>
-__global__ void __launch_bounds__(kStencilThreads)
-    k_stencil(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
-              KParams kp, const float* __restrict__ ctl, double* part_sum, double* part_max,
-              int16_t* argmin) {
-    typedef Ar<T> R;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int nctl = kp.nctl, nsub = kp.nsub, nchk = kp.nchk;
-    StencilSmem<T> sm = carve<T, EXACT>(smem_raw, nctl, nsub, nchk);
-    const Layout L = make_layout(kp);
-    GridT<T> g;
-    load_grid(g, kp.g);
-    const T cap = (T)kp.p.cap;
-
-    const int64_t pl = blockIdx.x / kp.tiles_x;
-    const int32_t xt = (int32_t)(blockIdx.x - pl * kp.tiles_x);
-    int32_t i3, i4, i5, i6;
-    {
-        int64_t q = pl;
-        i6 = (int32_t)(q % L.n[5]); q /= L.n[5];
-        i5 = (int32_t)(q % L.n[4]); q /= L.n[4];
-        i4 = (int32_t)(q % L.n[3]); q /= L.n[3];
-        i3 = (int32_t)q;
-    }
-
-    // Phase A: one thread per control integrates the held command from this
-    // plane's (h, v) -- the work the reference repeats for every (x, y).
-    if ((int)threadIdx.x < nchk) sm.aprobe[threadIdx.x] = R::div((T)(threadIdx.x + 1), (T)nchk);
-    for (int u = threadIdx.x; u < nctl; u += blockDim.x) {
-        ModelT<T> m;
-        load_model(m, kp.m);
-        State6<T> s;
-        s.x = g.lo[0];  // representative position: the dynamics never read it
-        s.y = g.lo[1];
-        s.h = axisvalue(g, 2, i3);
-        T vfx = axisvalue(g, 3, i4), vfy = axisvalue(g, 4, i5);
-        s.w = axisvalue(g, 5, i6);
-        T sh0, ch0;
-        R::sincos_(s.h, &sh0, &ch0);
-        s.vx = R::add(R::mul(ch0, vfx), R::mul(sh0, vfy));
-        s.vy = R::add(R::mul(-sh0, vfx), R::mul(ch0, vfy));
-        T tau0 = cfl_tau(g, m, vfx, vfy, s.w, kp.p);
-        int32_t ns = substeps_for(tau0, kp.p);
-        T incx[kStencilMaxSub], incy[kStencilMaxSub];
-        State6<T> ns6 = s;
-        bool ok = ns <= nsub &&
-                  integrate(m, ns6, (T)ctl[u], (T)ctl[u + nctl], (T)ctl[u + 2 * nctl], tau0, ns,
-                            kp.p.rk2 != 0, incx, incy);
-        for (int k = 0; k < nsub; ++k) {
-            sm.incx[k * nctl + u] = k < ns ? incx[k] : (T)0;
-            sm.incy[k * nctl + u] = k < ns ? incy[k] : (T)0;
-        }
-        sm.tau[u] = tau0;
-        T dh = R::sub(ns6.h, s.h);
-        ok = ok && finite_(R::sub(ns6.x, s.x)) && finite_(R::sub(ns6.y, s.y)) && finite_(dh) &&
-             finite_(ns6.vx) && finite_(ns6.vy) && finite_(ns6.w);
-        const T n3f = (T)g.n[2];
-        for (int sc = 0; sc < nchk; ++sc) {
-            int32_t ck = 0;
-            if (ok) {
-                T a = R::div((T)(sc + 1), (T)nchk);
-                T ph = R::add(s.h, R::mul(dh, a));
-                T gh = R::div(R::sub(ph, g.lo[2]), g.step[2]);
-                gh = R::sub(gh, R::mul(R::floor_(R::div(gh, n3f)), n3f));
-                ck = ((int32_t)R::rint_(gh)) % g.n[2];
-            }
-            sm.ck[sc * nctl + u] = ck;
-        }
-        int32_t jb[4] = {0, 0, 0, 0};
-        T tt[4] = {0, 0, 0, 0};
-        if (ok) {
-            T snh, cnh;
-            R::sincos_(ns6.h, &snh, &cnh);
-            T nvfx = R::sub(R::mul(cnh, ns6.vx), R::mul(snh, ns6.vy));
-            T nvfy = R::add(R::mul(snh, ns6.vx), R::mul(cnh, ns6.vy));
-            T f3 = R::div(R::sub(ns6.h, g.lo[2]), g.step[2]);
-            f3 = R::sub(f3, R::mul(R::floor_(R::div(f3, n3f)), n3f));
-            T f[4] = {f3, R::div(R::sub(nvfx, g.lo[3]), g.step[3]),
-                      R::div(R::sub(nvfy, g.lo[4]), g.step[4]),
-                      R::div(R::sub(ns6.w, g.lo[5]), g.step[5])};
-            ok = finite_(f[0]) && finite_(f[1]) && finite_(f[2]) && finite_(f[3]);
-            if (ok) {
-                for (int k = 1; k < 4; ++k) {
-                    T hi = (T)(g.n[2 + k] - 1);
-                    if (kp.p.vclamp) f[k] = jclamp(f[k], (T)0, hi);
-                    else if (f[k] < (T)0 || f[k] > hi) ok = false;
-                }
-            }
-            if (ok) {
-                for (int k = 0; k < 4; ++k) {
-                    T b = R::floor_(f[k]);
-                    tt[k] = R::sub(f[k], b);
-                    jb[k] = (int32_t)b;
-                }
-            }
-        }
-        sm.ok[u] = ok ? 1 : 0;
-        for (int c = 0; c < 16; ++c) {
-            const int c3 = c & 1, c4 = (c >> 1) & 1, c5 = (c >> 2) & 1, c6 = (c >> 3) & 1;
-            int32_t j3 = (jb[0] + c3) % g.n[2];
-            int32_t j4 = min(jb[1] + c4, g.n[3] - 1);
-            int32_t j5 = min(jb[2] + c5, g.n[4] - 1);
-            int32_t j6 = min(jb[3] + c6, g.n[5] - 1);
-            sm.plane[c * nctl + u] = ((j3 * g.n[3] + j4) * g.n[4] + j5) * g.n[5] + j6;
-            if (!EXACT) {
-                T w3 = c3 ? tt[0] : (T)1 - tt[0];
-                T w4 = c4 ? tt[1] : (T)1 - tt[1];
-                T w5 = c5 ? tt[2] : (T)1 - tt[2];
-                T w6 = c6 ? tt[3] : (T)1 - tt[3];
-                sm.w[c * nctl + u] = w3 * w4 * w5 * w6;
-            }
-        }
-        if (EXACT) {
-            for (int k = 0; k < 4; ++k) {
-                sm.w[(2 * k) * nctl + u] = R::sub((T)1, tt[k]);
-                sm.w[(2 * k + 1) * nctl + u] = tt[k];
-            }
-        }
-    }
-    __syncthreads();
-
-    // Phase B: every (x, y) cell of this tile scans all controls.
-    const int32_t n1 = L.n[0], n2 = L.n[1];
-    const int32_t x0 = (int32_t)xt * kp.tile_x;
-    const int32_t x1 = min(x0 + kp.tile_x, n1);
-    const int32_t ncell_tile = (x1 - x0) * n2;
-    const T lo0 = g.lo[0], lo1 = g.lo[1], st0 = g.step[0], st1 = g.step[1];
-    const T hx = (T)(n1 - 1), hy = (T)(n2 - 1);
-    const int64_t P = L.P;
-    const S* Vbase = Vin;
-    double dsum = 0.0, dmax = 0.0;
-    for (int c = threadIdx.x; c < ncell_tile; c += blockDim.x) {
-        const int32_t i1 = x0 + c / n2;
-        const int32_t i2 = c - (i1 - x0) * n2;
-        const int64_t didx = pl * P + (int64_t)i1 * n2 + i2;
-        const T old = (T)Conv<S>::ld(Vin + didx);
-        if (occ[L.occ(i1, i2, i3)]) {
-            Vout[didx] = Vin[didx];
-            if (argmin) argmin[L.rowmajor(i1, i2, i3, i4, i5, i6)] = -1;
-            continue;
-        }
-        const T x = axisvalue(g, 0, i1), y = axisvalue(g, 1, i2);
-        T best = cap;
-        int bk = 0;
-        for (int u = 0; u < nctl; ++u) {
-            T cval = cap;
-            if (sm.ok[u]) {
-                T xn = x, yn = y;
-                for (int k = 0; k < nsub; ++k) {
-                    xn = R::add(xn, sm.incx[k * nctl + u]);
-                    yn = R::add(yn, sm.incy[k * nctl + u]);
-                }
-                const T dx = R::sub(xn, x), dy = R::sub(yn, y);
-                bool hit = false;
-                for (int sc = 0; sc < nchk; ++sc) {
-                    const T a = sm.aprobe[sc];
-                    const T gx = R::div(R::sub(R::add(x, R::mul(dx, a)), lo0), st0);
-                    const T gy = R::div(R::sub(R::add(y, R::mul(dy, a)), lo1), st1);
-                    if (gx < (T)0 || gy < (T)0 || gx > hx || gy > hy) { hit = true; break; }
-                    const int32_t ci = (int32_t)R::rint_(gx), cj = (int32_t)R::rint_(gy);
-                    if (occ[L.occ(ci, cj, sm.ck[sc * nctl + u])]) { hit = true; break; }
-                }
-                if (!hit) {
-                    const T f1 = R::div(R::sub(xn, lo0), st0);
-                    const T f2 = R::div(R::sub(yn, lo1), st1);
-                    if (!(f1 < (T)0 || f1 > hx || f2 < (T)0 || f2 > hy)) {
-                        const T b1 = R::floor_(f1), b2 = R::floor_(f2);
-                        const T t1 = R::sub(f1, b1), t2 = R::sub(f2, b2);
-                        const int32_t j1 = (int32_t)b1, j2 = (int32_t)b2;
-                        const int32_t j1p = min(j1 + 1, n1 - 1), j2p = min(j2 + 1, n2 - 1);
-                        const int64_t o00 = (int64_t)j1 * n2 + j2, o01 = (int64_t)j1 * n2 + j2p;
-                        const int64_t o10 = (int64_t)j1p * n2 + j2, o11 = (int64_t)j1p * n2 + j2p;
-                        T acc = (T)0;
-                        if (EXACT) {
-                            // the reference's left-to-right weight products, corners
-                            // in its order (x fastest), one rounding per operation
-                            const T w1[2] = {R::sub((T)1, t1), t1};
-                            const T w2[2] = {R::sub((T)1, t2), t2};
-                            T p12[4];
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) p12[q] = R::mul(w1[q & 1], w2[q >> 1]);
-                            for (int hc = 0; hc < 16; ++hc) {
-                                const int c3 = hc & 1, c4 = (hc >> 1) & 1, c5 = (hc >> 2) & 1,
-                                          c6 = (hc >> 3) & 1;
-                                const T w3 = sm.w[(0 + c3) * nctl + u];
-                                const T w4 = sm.w[(2 + c4) * nctl + u];
-                                const T w5 = sm.w[(4 + c5) * nctl + u];
-                                const T w6 = sm.w[(6 + c6) * nctl + u];
-                                const S* Vp = Vbase + (int64_t)sm.plane[hc * nctl + u] * P;
-                                const T v[4] = {(T)Conv<S>::ld(Vp + o00), (T)Conv<S>::ld(Vp + o10),
-                                                (T)Conv<S>::ld(Vp + o01), (T)Conv<S>::ld(Vp + o11)};
-#pragma unroll
-                                for (int q = 0; q < 4; ++q) {
-                                    T wgt = R::mul(R::mul(R::mul(R::mul(p12[q], w3), w4), w5), w6);
-                                    if (wgt != (T)0) acc = R::add(acc, R::mul(wgt, v[q]));
-                                }
-                            }
-                        } else {
-                            const T u1 = (T)1 - t1, u2 = (T)1 - t2;
-                            for (int hc = 0; hc < 16; ++hc) {
-                                const S* Vp = Vbase + (int64_t)sm.plane[hc * nctl + u] * P;
-                                const T v00 = (T)Conv<S>::ld(Vp + o00), v01 = (T)Conv<S>::ld(Vp + o01);
-                                const T v10 = (T)Conv<S>::ld(Vp + o10), v11 = (T)Conv<S>::ld(Vp + o11);
-                                const T sxy = u1 * (u2 * v00 + t2 * v01) + t1 * (u2 * v10 + t2 * v11);
-                                acc += sm.w[hc * nctl + u] * sxy;
-                            }
-                        }
-                        const T nv = jmin(acc, cap);
-                        cval = jmin(R::add(sm.tau[u], nv), cap);
-                    }
-                }
-            }
-            if (u == 0) { best = cval; bk = 0; }
-            else if (cval < best) { best = cval; bk = u; }
-        }
-        if (argmin) argmin[L.rowmajor(i1, i2, i3, i4, i5, i6)] = (int16_t)bk;
-        if (best < old) {
-            const S nv = Conv<S>::template st<T>(best);
-            const T nvT = (T)Conv<S>::val(nv);
-            Vout[didx] = nv;
-            const double d = (double)old - (double)nvT;
-            dsum += d;
-            dmax = fmax(dmax, d);
-        } else {
-            Vout[didx] = Vin[didx];
-        }
-    }
-    block_partial(dsum, dmax, part_sum, part_max);
-}
+#include "pg_stencil.cuh"
 
 // ---------------------------------------------------------------------------
 // Encoding (encode_into!, Pipeline.jl:698-780), from the device layout into
@@ -1001,33 +738,43 @@ size_t stencil_smem(int storage, bool exact, const KParams& kp) {
                  : stencil_smem_bytes<float, false>(kp.nctl, kp.nsub, kp.nchk);
 }
 
-template <typename S, typename T, bool EXACT>
+template <typename S, typename T, bool EXACT, int NSUB>
 static cudaError_t stencil_t(const void* Vin, void* Vout, const uint8_t* occ, const KParams& kp,
-                             const float* ctl, const SweepBufs& sb, int16_t* argmin,
-                             cudaStream_t st, int64_t* launches) {
+                             const float* ctl, const int32_t* order, const SweepBufs& sb,
+                             int16_t* argmin, cudaStream_t st, int64_t* launches) {
     const int64_t blocks = stencil_blocks(kp);
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const size_t smem = stencil_smem_bytes<T, EXACT>(kp.nctl, kp.nsub, kp.nchk);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_stencil<S, T, EXACT>,
+        cudaError_t e = cudaFuncSetAttribute(k_stencil<S, T, EXACT, NSUB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    k_stencil<S, T, EXACT><<<(unsigned)blocks, kStencilThreads, smem, st>>>(
-        (const S*)Vin, (S*)Vout, occ, kp, ctl, sb.part_sum, sb.part_max, argmin);
+    k_stencil<S, T, EXACT, NSUB><<<(unsigned)blocks, kp.block, smem, st>>>(
+        (const S*)Vin, (S*)Vout, occ, kp, ctl, order, sb.part_sum, sb.part_max, argmin);
     k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
     *launches += 2;
     return cudaGetLastError();
 }
 
+template <typename S, typename T, bool EXACT>
+static cudaError_t stencil_n(const void* Vin, void* Vout, const uint8_t* occ, const KParams& kp,
+                             const float* ctl, const int32_t* order, const SweepBufs& sb,
+                             int16_t* argmin, cudaStream_t st, int64_t* launches) {
+    if (kp.nsub == 5)
+        return stencil_t<S, T, EXACT, 5>(Vin, Vout, occ, kp, ctl, order, sb, argmin, st, launches);
+    return stencil_t<S, T, EXACT, 0>(Vin, Vout, occ, kp, ctl, order, sb, argmin, st, launches);
+}
+
 cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout, const uint8_t* occ,
-                           const KParams& kp, const float* ctl, const SweepBufs& sb,
-                           int16_t* argmin, cudaStream_t st, int64_t* launches) {
-#define PG_ST(S, T)                                                                           \
-    return exact ? stencil_t<S, T, true>(Vin, Vout, occ, kp, ctl, sb, argmin, st, launches)     \
-                 : stencil_t<S, T, false>(Vin, Vout, occ, kp, ctl, sb, argmin, st, launches)
+                           const KParams& kp, const float* ctl, const int32_t* order,
+                           const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                           int64_t* launches) {
+#define PG_ST(S, T)                                                                               \
+    return exact ? stencil_n<S, T, true>(Vin, Vout, occ, kp, ctl, order, sb, argmin, st, launches) \
+                 : stencil_n<S, T, false>(Vin, Vout, occ, kp, ctl, order, sb, argmin, st, launches)
     switch (storage) {
         case PG_STORE_F32: PG_ST(float, float);
         case PG_STORE_F16: PG_ST(__half, float);

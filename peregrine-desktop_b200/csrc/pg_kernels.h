@@ -27,8 +27,8 @@ cudaError_t launch_cellform(int storage, bool esc, const void* Vin, void* Vout,
                             int64_t* launches);
 cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout,
                            const uint8_t* occ, const KParams& kp, const float* ctl,
-                           const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
-                           int64_t* launches);
+                           const int32_t* order, const SweepBufs& sb, int16_t* argmin,
+                           cudaStream_t st, int64_t* launches);
 cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t dtype,
                           double scale, double escape_scale, int64_t lo, int64_t n, uint8_t* out,
                           unsigned long long* counts, cudaStream_t st);

@@ -10,7 +10,7 @@ namespace pg {
 // Largest substep count / probe count the stencil kernel stages in shared
 // memory.  Schemes beyond these run on the cell-form kernel.
 constexpr int kStencilMaxSub = 16;
-constexpr int kStencilMaxChk = 24;
+constexpr int kStencilMaxChk = 4;
 constexpr int kStencilThreads = 256;
 constexpr int kCellThreads = 128;
 
@@ -27,6 +27,7 @@ struct KParams {
     int32_t tiles_x;  // stencil: blocks per plane
     int32_t nsub;     // stencil: substeps of the single horizon
     int32_t nchk;     // stencil: swept probes per lookahead
+    int32_t block;    // stencil: threads per block
     int32_t phase;
 };
 

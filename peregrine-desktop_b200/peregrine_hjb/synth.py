@@ -32,6 +32,9 @@ WORKLOADS = {
     "tiny": dict(n=[12, 12, 8, 5, 5, 5], control_set="cube3", dt=0.05, rects=2),
     "small": dict(n=[24, 24, 16, 9, 9, 9], control_set="cube3", dt=0.05, rects=3),
     "medium": dict(n=[48, 48, 32, 15, 15, 15], control_set="cube5", dt=0.04, rects=6),
+    # the medium workload's planes and controls with a quarter of the headings:
+    # the same per-block work, small enough for a profiler capture
+    "medium_h8": dict(n=[48, 48, 8, 15, 15, 15], control_set="cube5", dt=0.04, rects=6),
     "large": dict(n=[96, 96, 64, 21, 21, 21], control_set="cube5", dt=0.03, rects=8),
 }
 

@@ -38,7 +38,9 @@ def card_value(root, m, t, subs):
         raw = fh.read(eb)
     if enc["dtype"] == "u16":
         r = int.from_bytes(raw, "little")
-        return math.inf if r >= enc["escape_base"] or r == 65535 else r * enc["scale"]
+        if r == enc["unreachable"] or (enc["escape_codes"] and r >= enc["escape_base"]):
+            return math.inf
+        return r * enc["scale"]
     return float(np.frombuffer(raw, np.float32)[0])
 
 

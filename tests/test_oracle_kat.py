@@ -276,3 +276,23 @@ def test_target_cells_nearest_fallback(og):
     half = [float(g.step[k]) * 0.5 for k in range(6)]
     many = og.target_cells(g, (30.0, 40.0, 0.0, 0, 0, 0), half)
     assert len(many) >= 1
+
+
+def test_golden_fixed_point_is_a_fixed_point(og):
+    """tests/golden/tiny_fixed_point.npz (made by make_golden.py from the
+    oracle) really is the oracle's converged table: one more oracle sweep
+    moves no cell by more than the 1e-4 s stop tolerance, and its argmin is
+    the one stored."""
+    import os
+    from peregrine_hjb.synth import Problem
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "tiny_fixed_point.npz"))
+    pr = Problem("tiny", seed=5)
+    g = og.copy_struct(pr.grid.to_c(), og.OGrid)
+    m = og.copy_struct(pr.model.to_c(), og.OModel)
+    p = og.copy_struct(pr.params, og.OParams)
+    V = gold["V"]
+    assert V.shape == (pr.ncells,) and np.all(V[pr.seeds] == 0)
+    _, _, mx, am = og.sweep_jacobi(V, pr.occ, g, m, pr.ctl, p, phase=int(gold["iterations"]),
+                                   argmin=True)
+    assert mx <= 1e-4
+    assert np.array_equal(am, gold["argmin"])
