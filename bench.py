@@ -309,6 +309,50 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def run_accuracy(args, local_rank):
+    """Time-to-converge and precision report: the same table solved to the
+    max-norm stop (1e-4 s) with FP32 storage, FP64 (the device oracle), and
+    FP16 / BF16 storage followed by FP32 polish sweeps; errors of each against
+    FP64 and FP32."""
+    import numpy as np
+    import torch
+    from peregrine_hjb import _lib
+
+    torch.cuda.set_device(local_rank)
+    pr = problem_for_rank(0)
+    args_c = (pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.seeds, pr.ctl,
+              args.max_sweeps, 1e-4)
+    runs = {}
+    tables = {}
+    for name, kw in (("fp32", dict(storage="fp32")), ("fp64", dict(storage="fp64")),
+                     ("fp16", dict(storage="fp16", polish_sweeps=args.max_sweeps)),
+                     ("bf16", dict(storage="bf16", polish_sweeps=args.max_sweeps))):
+        if name not in args.storages.split(","):
+            continue
+        opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL, **kw)
+        V, res = _lib.solve_value(*args_c, opts, device=local_rank)
+        tables[name] = V
+        runs[name] = {"sweeps": res.iterations, "polish_sweeps": res.polish_iterations,
+                      "kernel_s": res.kernel_ms / 1000.0, "wall_s": res.elapsed_ms / 1000.0,
+                      "last_maxnorm": res.last_maxnorm}
+    ref = tables.get("fp64", tables.get("fp32"))
+    reached = ref < np.float32(pr.params.cap) - 1e-3
+    for name, V in tables.items():
+        d = np.abs(V.astype(np.float64) - ref.astype(np.float64))
+        runs[name]["max_abs_err_vs_" + ("fp64" if "fp64" in tables else "fp32")] = float(d.max())
+        runs[name]["rms_err_reached"] = float(np.sqrt(np.mean(d[reached] ** 2))) if reached.any() else 0.0
+        if "fp32" in tables and name != "fp32":
+            runs[name]["max_abs_err_vs_fp32"] = float(np.max(np.abs(V - tables["fp32"])))
+    line = {"report": "accuracy", "workload": WORKLOAD, "cells": pr.ncells, "controls": pr.nctl,
+            "stop": "max-norm residual < 1e-4 s", "runs": runs}
+    if "fp32" in runs:
+        for name in ("fp16", "bf16"):
+            if name in runs:
+                runs[name]["speedup_vs_fp32"] = runs["fp32"]["kernel_s"] / runs[name]["kernel_s"]
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -321,6 +365,11 @@ def main():
     ap.add_argument("--only-device", action="store_true",
                     help="time the device sweeps only (no end-to-end leg, no CPU baseline); "
                          "for profiler captures")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="time-to-converge and FP32/FP64/FP16/BF16 error report instead of "
+                         "the throughput line")
+    ap.add_argument("--storages", default="fp32,fp64,fp16,bf16")
+    ap.add_argument("--max-sweeps", type=int, default=4000)
     args = ap.parse_args()
     globals()["WORKLOAD"] = args.workload
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -328,6 +377,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.accuracy:
+        return run_accuracy(args, local_rank)
     if world > 1:
         import datetime
         import torch

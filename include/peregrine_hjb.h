@@ -101,6 +101,7 @@ typedef struct pg_params {
 #define PG_KERNEL_STENCIL  1  /* position-invariant stencil (plain scheme)     */
 #define PG_KERNEL_CELLFORM 2  /* one thread per cell, the full cell_update     */
 #define PG_KERNEL_STENCIL_EXACT 3 /* stencil with the reference's rounding order */
+#define PG_KERNEL_STENCIL_ROWS  4 /* stencil deciding every probe per sweep (no mask) */
 
 /* Table dtypes (solver/src/Pipeline.jl:620-625). */
 #define PG_DTYPE_U8  0

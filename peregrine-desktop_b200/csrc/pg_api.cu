@@ -78,6 +78,8 @@ struct pg_ctx {
     float* ctl_d = nullptr;
     int32_t* order_d = nullptr;
     std::vector<int32_t> order_h;
+    uint32_t* mask_d = nullptr;  // admissibility bits of the masked stencil
+    bool mask_ok = false;
     int8_t* pol_d = nullptr;
     double* part_sum = nullptr;
     double* part_max = nullptr;
@@ -106,6 +108,9 @@ struct pg_ctx {
         if (ctl_d) cudaFree(ctl_d);
         if (order_d) cudaFree(order_d);
         order_d = nullptr;
+        if (mask_d) cudaFree(mask_d);
+        mask_d = nullptr;
+        mask_ok = false;
         if (pol_d) cudaFree(pol_d);
         if (part_sum) cudaFree(part_sum);
         if (part_max) cudaFree(part_max);
@@ -165,7 +170,9 @@ int pick_kernel(pg_ctx* ctx, int32_t kernel, int* out) {
     if (kernel == PG_KERNEL_AUTO) kernel = ctx->stencil_ok ? PG_KERNEL_STENCIL : PG_KERNEL_CELLFORM;
     if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_EXACT) && !ctx->stencil_ok)
         return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
-    if (kernel < PG_KERNEL_STENCIL || kernel > PG_KERNEL_STENCIL_EXACT)
+    if (kernel == PG_KERNEL_STENCIL_ROWS && !ctx->stencil_ok)
+        return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
+    if (kernel < PG_KERNEL_STENCIL || kernel > PG_KERNEL_STENCIL_ROWS)
         return fail(PG_EINVAL, "unknown kernel " + std::to_string(kernel));
     *out = kernel;
     return PG_OK;
@@ -183,6 +190,10 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
         e = pg::launch_cellform(ctx->storage, esc, vin, vout, ctx->occ_d,
                                 use_pol ? ctx->pol_d : nullptr, ctx->kp, ctx->ctl_d, sb, argmin_d,
                                 ctx->stream, &ctx->launches);
+    else if (kernel == PG_KERNEL_STENCIL && ctx->mask_ok && ctx->storage != PG_STORE_F64)
+        e = pg::launch_stencil_u(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->kp,
+                                 ctx->ctl_d, ctx->order_d, sb, argmin_d, ctx->stream,
+                                 &ctx->launches);
     else
         e = pg::launch_stencil(ctx->storage, kernel == PG_KERNEL_STENCIL_EXACT, vin, vout,
                                ctx->occ_d, ctx->kp, ctx->ctl_d, ctx->order_d, sb, argmin_d,
@@ -365,6 +376,27 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
         }
         kp.block = best_bs;
     }
+    // Masked stencil: blocks of 2 rows x 4 columns per thread, whole planes
+    // per block up to 2048 such blocks.
+    {
+        const int64_t rbn = (g->n[0] + 1) / 2, cbn = (g->n[1] + 3) / 4;
+        const int64_t ntile = (rbn * cbn + 2047) / 2048;
+        const int32_t rows_per_tile = (int32_t)(2 * ((rbn + ntile - 1) / ntile));
+        kp.utile_x = rows_per_tile;
+        kp.utiles_x = (g->n[0] + rows_per_tile - 1) / rows_per_tile;
+        const int64_t segs = (int64_t)((rows_per_tile + 1) / 2) * cbn;
+        int best_bs = 256;
+        int64_t best_waste = -1;
+        if (segs < 96) {
+            best_bs = (int)(32 * ((segs + 31) / 32));
+        } else {
+            for (int bs = 256; bs >= 96; bs -= 32) {
+                const int64_t waste = ((segs + bs - 1) / bs) * bs - segs;
+                if (best_waste < 0 || waste < best_waste) { best_waste = waste; best_bs = bs; }
+            }
+        }
+        kp.ublock = best_bs;
+    }
     kp.nsub = host_substeps_for(p->cfl <= 0.0f ? p->dt : p->tau_max, *p);
     kp.nchk = p->checks;
 
@@ -421,8 +453,27 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     ctx->nparts = pg::cellform_blocks(kp.ncells);
     const int64_t sb = pg::stencil_blocks(kp);
     if (sb > ctx->nparts) ctx->nparts = sb;
+    const int64_t ub = kp.nplanes * kp.utiles_x;
+    if (ub > ctx->nparts) ctx->nparts = ub;
     PG_CUDA(cudaMalloc(&ctx->part_sum, sizeof(double) * ctx->nparts));
     PG_CUDA(cudaMalloc(&ctx->part_max, sizeof(double) * ctx->nparts));
+    // The admissibility mask of the masked stencil: decided once here, read by
+    // every sweep.  Skipped (the row stencil decides per sweep instead) when
+    // it would not leave 4 GiB of device memory free.
+    if (ctx->stencil_ok && storage != PG_STORE_F64) {
+        const size_t mb = pg::stencil_mask_bytes(kp);
+        size_t fr = 0, tot = 0;
+        PG_CUDA(cudaMemGetInfo(&fr, &tot));
+        if (mb + ((size_t)4 << 30) < fr && cudaMalloc(&ctx->mask_d, mb) == cudaSuccess) {
+            cudaError_t e = pg::launch_stencil_mask(ctx->occ_d, kp, ctx->ctl_d, ctx->mask_d,
+                                                    ctx->stream, &ctx->launches);
+            if (e != cudaSuccess) return fail(PG_ECUDA, std::string("mask: ") + cudaGetErrorString(e));
+            ctx->mask_ok = true;
+        } else {
+            cudaGetLastError();
+            ctx->mask_d = nullptr;
+        }
+    }
     PG_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->loaded = true;
     return PG_OK;
@@ -500,9 +551,15 @@ int pg_solve(pg_ctx* ctx, const int64_t* tidx, int64_t ntidx, int32_t iters, dou
         ctx->storage = PG_STORE_F32;
         double d2 = d, dm2 = dm;
         bool conv2 = false;
+        // Plain value iteration (V <- T V) for the polish: the 16-bit table's
+        // rounding error has both signs, and a cell rounded below the fixed
+        // point must be allowed back up (stencil kernels; the cell-form
+        // kernel keeps the reference's lower-only update).
+        ctx->kp.relax = 1;
         rc = iterate(ctx, kernel, false, opts.polish_sweeps, tol, opts.stop_rule,
                      opts.warm_start != 0, opts.progress_every, done, cb, user, &pdone, &d2, &dm2,
                      &kms, &conv2);
+        ctx->kp.relax = 0;
         if (rc) return rc;
         d = d2;
         dm = dm2;

@@ -33,16 +33,16 @@
 
 namespace pg {
 
-// 16-bit storage rounds UP.  Value iteration here only ever lowers a cell,
-// so a stored value must stay an upper bound of the FP32 iterate: a value
-// rounded to nearest can land below the fixed point, and no later sweep (16-
-// or 32-bit) can raise it again.  Rounded up, the 16-bit phase stops at or
-// above the FP32 fixed point and the FP32 polish sweeps descend onto it.
+// 16-bit storage rounds to nearest.  A step of 0.03-0.05 s is only a few
+// FP16 ulps at 16-32 s, so any directed rounding accumulates along a route
+// of hundreds of steps; round-to-nearest keeps the error zero-mean, and the
+// FP32 polish that follows a 16-bit solve (plain value iteration, V <- T V,
+// see KParams::relax) removes it.
 template <> struct Conv<__half> {
     static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
     static __device__ __forceinline__ float val(__half v) { return __half2float(v); }
     template <typename T> static __device__ __forceinline__ __half st(T v) {
-        return __float2half_ru((float)v);
+        return __float2half_rn((float)v);
     }
 };
 template <> struct Conv<__nv_bfloat16> {
@@ -51,7 +51,7 @@ template <> struct Conv<__nv_bfloat16> {
     }
     static __device__ __forceinline__ float val(__nv_bfloat16 v) { return __bfloat162float(v); }
     template <typename T> static __device__ __forceinline__ __nv_bfloat16 st(T v) {
-        return __float2bfloat16_ru((float)v);
+        return __float2bfloat16_rn((float)v);
     }
 };
 
@@ -550,7 +550,9 @@ __global__ void __launch_bounds__(kCellThreads)
     block_partial(dsum, dmax, part_sum, part_max);
 }
 
+#include "pg_plane.cuh"
 #include "pg_stencil.cuh"
+#include "pg_stencil_u.cuh"
 
 // ---------------------------------------------------------------------------
 // Encoding (encode_into!, Pipeline.jl:698-780), from the device layout into
@@ -783,6 +785,72 @@ cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout,
     }
 #undef PG_ST
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_stencil_mask(const uint8_t* occ, const KParams& kp, const float* ctl,
+                                uint32_t* mask, cudaStream_t st, int64_t* launches) {
+    const size_t smem = stencil_mask_smem(kp.nctl, kp.nsub);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_mask<float>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_stencil_mask<float><<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+// columns per thread of the masked stencil: one 16-byte vector of storage
+template <typename S> struct UStencilR { static constexpr int R = 4; };
+template <> struct UStencilR<__half> { static constexpr int R = 8; };
+template <> struct UStencilR<__nv_bfloat16> { static constexpr int R = 8; };
+
+template <typename S>
+static cudaError_t stencil_u_t(const void* Vin, void* Vout, const uint8_t* occ,
+                               const uint32_t* mask, const KParams& kp, const float* ctl,
+                               const int32_t* order, const SweepBufs& sb, int16_t* argmin,
+                               cudaStream_t st, int64_t* launches) {
+    KParams ku = kp;
+    ku.tile_x = kp.utile_x;
+    ku.tiles_x = kp.utiles_x;
+    const int64_t blocks = kp.nplanes * kp.utiles_x;
+    if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const size_t smem = stencil_u_smem(kp.nctl);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_u<S, kURX, UStencilR<S>::R>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_stencil_u<S, kURX, UStencilR<S>::R><<<(unsigned)blocks, kp.ublock, smem, st>>>(
+        (const S*)Vin, (S*)Vout, occ, mask, ku, ctl, order, sb.part_sum, sb.part_max, argmin);
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil_u(int storage, const void* Vin, void* Vout, const uint8_t* occ,
+                             const uint32_t* mask, const KParams& kp, const float* ctl,
+                             const int32_t* order, const SweepBufs& sb, int16_t* argmin,
+                             cudaStream_t st, int64_t* launches) {
+    switch (storage) {
+        case PG_STORE_F32:
+            return stencil_u_t<float>(Vin, Vout, occ, mask, kp, ctl, order, sb, argmin, st, launches);
+        case PG_STORE_F16:
+            return stencil_u_t<__half>(Vin, Vout, occ, mask, kp, ctl, order, sb, argmin, st, launches);
+        case PG_STORE_BF16:
+            return stencil_u_t<__nv_bfloat16>(Vin, Vout, occ, mask, kp, ctl, order, sb, argmin, st,
+                                              launches);
+    }
+    return cudaErrorInvalidValue;
+}
+
+size_t stencil_mask_bytes(const KParams& kp) {
+    return (size_t)kp.nplanes * kp.nctl * kp.g.n[0] * mask_words(kp.g.n[1]) * sizeof(uint32_t);
 }
 
 cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t dtype,

@@ -148,92 +148,23 @@ __global__ void __launch_bounds__(256)
         ord[u] = order[u];
         T* rec = rt + (size_t)u * RL.NT;
         int32_t* irec = ri + (size_t)u * RL.NI;
-        ModelT<T> m;
-        load_model(m, kp.m);
-        State6<T> s;
-        s.x = g.lo[0];  // representative position: the dynamics never read it
-        s.y = g.lo[1];
-        s.h = axisvalue(g, 2, i3);
-        const T vfx = axisvalue(g, 3, i4), vfy = axisvalue(g, 4, i5);
-        s.w = axisvalue(g, 5, i6);
-        T sh0, ch0;
-        R_::sincos_(s.h, &sh0, &ch0);
-        s.vx = R_::add(R_::mul(ch0, vfx), R_::mul(sh0, vfy));
-        s.vy = R_::add(R_::mul(-sh0, vfx), R_::mul(ch0, vfy));
-        const T tau0 = cfl_tau(g, m, vfx, vfy, s.w, kp.p);
-        const int32_t ns = substeps_for(tau0, kp.p);
-        T incx[kStencilMaxSub], incy[kStencilMaxSub];
-        State6<T> e = s;
-        bool ok = ns == nsub && integrate(m, e, (T)ctl[u], (T)ctl[u + nctl],
-                                          (T)ctl[u + 2 * nctl], tau0, ns, kp.p.rk2 != 0, incx, incy);
+        Transition<T> t;
+        transition(kp, g, i3, i4, i5, i6, ctl, u, t);
         for (int k = 0; k < nsub; ++k) {
-            rec[RL.incx(k)] = ok ? incx[k] : (T)0;
-            rec[RL.incy(k)] = ok ? incy[k] : (T)0;
+            rec[RL.incx(k)] = t.incx[k];
+            rec[RL.incy(k)] = t.incy[k];
         }
-        rec[RL.TAU] = tau0;
-        const T dh = R_::sub(e.h, s.h);
-        ok = ok && finite_(R_::sub(e.x, s.x)) && finite_(R_::sub(e.y, s.y)) && finite_(dh) &&
-             finite_(e.vx) && finite_(e.vy) && finite_(e.w);
-        const T n3f = (T)g.n[2];
-        for (int sc = 0; sc < nchk; ++sc) {
-            int32_t ck = 0;
-            if (ok) {
-                const T a = R_::div((T)(sc + 1), (T)nchk);
-                const T ph = R_::add(s.h, R_::mul(dh, a));
-                T gh = R_::div(R_::sub(ph, g.lo[2]), g.step[2]);
-                gh = R_::sub(gh, R_::mul(R_::floor_(R_::div(gh, n3f)), n3f));
-                ck = ((int32_t)R_::rint_(gh)) % g.n[2];
-            }
-            irec[RL.ck(sc)] = ck;
-        }
-        int32_t jb[4] = {0, 0, 0, 0};
-        T tt[4] = {0, 0, 0, 0};
-        if (ok) {
-            T snh, cnh;
-            R_::sincos_(e.h, &snh, &cnh);
-            const T nvfx = R_::sub(R_::mul(cnh, e.vx), R_::mul(snh, e.vy));
-            const T nvfy = R_::add(R_::mul(snh, e.vx), R_::mul(cnh, e.vy));
-            T f3 = R_::div(R_::sub(e.h, g.lo[2]), g.step[2]);
-            f3 = R_::sub(f3, R_::mul(R_::floor_(R_::div(f3, n3f)), n3f));
-            T f[4] = {f3, R_::div(R_::sub(nvfx, g.lo[3]), g.step[3]),
-                      R_::div(R_::sub(nvfy, g.lo[4]), g.step[4]),
-                      R_::div(R_::sub(e.w, g.lo[5]), g.step[5])};
-            ok = finite_(f[0]) && finite_(f[1]) && finite_(f[2]) && finite_(f[3]);
-            if (ok) {
-                for (int k = 1; k < 4; ++k) {
-                    const T hi = (T)(g.n[2 + k] - 1);
-                    if (kp.p.vclamp) f[k] = jclamp(f[k], (T)0, hi);
-                    else if (f[k] < (T)0 || f[k] > hi) ok = false;
-                }
-            }
-            if (ok) {
-                for (int k = 0; k < 4; ++k) {
-                    const T b = R_::floor_(f[k]);
-                    tt[k] = R_::sub(f[k], b);
-                    jb[k] = (int32_t)b;
-                }
-            }
-        }
-        irec[RL.OK] = ok ? 1 : 0;
+        rec[RL.TAU] = t.tau;
+        for (int sc = 0; sc < nchk; ++sc) irec[RL.ck(sc)] = t.ck[sc];
+        irec[RL.OK] = t.ok ? 1 : 0;
         for (int c = 0; c < 16; ++c) {
-            const int c3 = c & 1, c4 = (c >> 1) & 1, c5 = (c >> 2) & 1, c6 = (c >> 3) & 1;
-            const int32_t j3 = (jb[0] + c3) % g.n[2];
-            const int32_t j4 = min(jb[1] + c4, g.n[3] - 1);
-            const int32_t j5 = min(jb[2] + c5, g.n[4] - 1);
-            const int32_t j6 = min(jb[3] + c6, g.n[5] - 1);
-            irec[RL.PLANE + c] = ((j3 * g.n[3] + j4) * g.n[4] + j5) * g.n[5] + j6;
-            if (!EXACT) {
-                const T w3 = c3 ? tt[0] : (T)1 - tt[0];
-                const T w4 = c4 ? tt[1] : (T)1 - tt[1];
-                const T w5 = c5 ? tt[2] : (T)1 - tt[2];
-                const T w6 = c6 ? tt[3] : (T)1 - tt[3];
-                rec[RL.W + c] = w3 * w4 * w5 * w6;
-            }
+            irec[RL.PLANE + c] = corner_plane(g, t, c);
+            if (!EXACT) rec[RL.W + c] = corner_weight(t, c);
         }
         if (EXACT) {
             for (int k = 0; k < 4; ++k) {
-                rec[RL.W + 2 * k] = R_::sub((T)1, tt[k]);
-                rec[RL.W + 2 * k + 1] = tt[k];
+                rec[RL.W + 2 * k] = R_::sub((T)1, t.tt[k]);
+                rec[RL.W + 2 * k + 1] = t.tt[k];
             }
             for (int k = 8; k < 16; ++k) rec[RL.W + k] = (T)0;
         }
@@ -491,11 +422,11 @@ __global__ void __launch_bounds__(256)
                 continue;
             }
             if (argmin) argmin[L.rowmajor(i1, j, i3, i4, i5, i6)] = (int16_t)bk[r];
-            if (best[r] < old[r]) {
+            if (best[r] < old[r] || (kp.relax && best[r] != old[r])) {
                 const S nv = Conv<S>::template st<T>(best[r]);
                 const T nvT = (T)Conv<S>::val(nv);
                 Vout[didx] = nv;
-                const double d = (double)old[r] - (double)nvT;
+                const double d = fabs((double)old[r] - (double)nvT);
                 dsum += d;
                 dmax = fmax(dmax, d);
             } else {

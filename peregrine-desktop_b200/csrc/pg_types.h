@@ -28,6 +28,10 @@ struct KParams {
     int32_t nsub;     // stencil: substeps of the single horizon
     int32_t nchk;     // stencil: swept probes per lookahead
     int32_t block;    // stencil: threads per block
+    int32_t utile_x;  // masked stencil: x rows per block
+    int32_t utiles_x; // masked stencil: blocks per plane
+    int32_t ublock;   // masked stencil: threads per block
+    int32_t relax;    // 0: V' = min(V, T V), the reference's update; 1: V' = T V
     int32_t phase;
 };
 
