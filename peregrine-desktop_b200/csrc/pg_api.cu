@@ -79,6 +79,7 @@ struct pg_ctx {
     int32_t* order_d = nullptr;
     std::vector<int32_t> order_h;
     uint32_t* mask_d = nullptr;  // admissibility bits of the masked stencil
+    uint32_t* recs_d = nullptr;  // its per-(plane, control) records
     bool mask_ok = false;
     int8_t* pol_d = nullptr;
     double* part_sum = nullptr;
@@ -110,6 +111,8 @@ struct pg_ctx {
         order_d = nullptr;
         if (mask_d) cudaFree(mask_d);
         mask_d = nullptr;
+        if (recs_d) cudaFree(recs_d);
+        recs_d = nullptr;
         mask_ok = false;
         if (pol_d) cudaFree(pol_d);
         if (part_sum) cudaFree(part_sum);
@@ -191,8 +194,8 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
                                 use_pol ? ctx->pol_d : nullptr, ctx->kp, ctx->ctl_d, sb, argmin_d,
                                 ctx->stream, &ctx->launches);
     else if (kernel == PG_KERNEL_STENCIL && ctx->mask_ok && ctx->storage != PG_STORE_F64)
-        e = pg::launch_stencil_u(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->kp,
-                                 ctx->ctl_d, ctx->order_d, sb, argmin_d, ctx->stream,
+        e = pg::launch_stencil_u(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
+                                 ctx->kp, ctx->order_d, sb, argmin_d, ctx->stream,
                                  &ctx->launches);
     else
         e = pg::launch_stencil(ctx->storage, kernel == PG_KERNEL_STENCIL_EXACT, vin, vout,
@@ -461,17 +464,20 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     // every sweep.  Skipped (the row stencil decides per sweep instead) when
     // it would not leave 4 GiB of device memory free.
     if (ctx->stencil_ok && storage != PG_STORE_F64) {
-        const size_t mb = pg::stencil_mask_bytes(kp);
+        const size_t mb = pg::stencil_mask_bytes(kp), rb = pg::stencil_recs_bytes(kp);
         size_t fr = 0, tot = 0;
         PG_CUDA(cudaMemGetInfo(&fr, &tot));
-        if (mb + ((size_t)4 << 30) < fr && cudaMalloc(&ctx->mask_d, mb) == cudaSuccess) {
-            cudaError_t e = pg::launch_stencil_mask(ctx->occ_d, kp, ctx->ctl_d, ctx->mask_d,
-                                                    ctx->stream, &ctx->launches);
-            if (e != cudaSuccess) return fail(PG_ECUDA, std::string("mask: ") + cudaGetErrorString(e));
+        if (mb + rb + ((size_t)4 << 30) < fr && cudaMalloc(&ctx->mask_d, mb) == cudaSuccess &&
+            cudaMalloc(&ctx->recs_d, rb) == cudaSuccess) {
+            cudaError_t e = pg::launch_stencil_prep(ctx->occ_d, kp, ctx->ctl_d, ctx->mask_d,
+                                                    ctx->recs_d, ctx->stream, &ctx->launches);
+            if (e != cudaSuccess) return fail(PG_ECUDA, std::string("prep: ") + cudaGetErrorString(e));
             ctx->mask_ok = true;
         } else {
             cudaGetLastError();
+            if (ctx->mask_d) cudaFree(ctx->mask_d);
             ctx->mask_d = nullptr;
+            ctx->recs_d = nullptr;
         }
     }
     PG_CUDA(cudaStreamSynchronize(ctx->stream));

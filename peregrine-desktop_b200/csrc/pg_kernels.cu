@@ -787,32 +787,34 @@ cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout,
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_stencil_mask(const uint8_t* occ, const KParams& kp, const float* ctl,
-                                uint32_t* mask, cudaStream_t st, int64_t* launches) {
-    const size_t smem = stencil_mask_smem(kp.nctl, kp.nsub);
+cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const float* ctl,
+                                uint32_t* mask, uint32_t* recs, cudaStream_t st,
+                                int64_t* launches) {
+    const size_t smem = stencil_prep_smem(kp.nctl, kp.nsub);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_stencil_mask<float>,
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_prep,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     if (kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
-    k_stencil_mask<float><<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask);
+    k_stencil_prep<<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask, recs);
     *launches += 1;
     return cudaGetLastError();
 }
 
-// columns per thread of the masked stencil: one 16-byte vector of storage
+// columns per thread of the masked stencil: a multiple of one 16-byte vector
 template <typename S> struct UStencilR { static constexpr int R = 4; };
 template <> struct UStencilR<__half> { static constexpr int R = 8; };
 template <> struct UStencilR<__nv_bfloat16> { static constexpr int R = 8; };
 
-template <typename S>
+template <typename S, bool ARGMIN>
 static cudaError_t stencil_u_t(const void* Vin, void* Vout, const uint8_t* occ,
-                               const uint32_t* mask, const KParams& kp, const float* ctl,
+                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                                const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                                cudaStream_t st, int64_t* launches) {
+    constexpr int R = UStencilR<S>::R;
     KParams ku = kp;
     ku.tile_x = kp.utile_x;
     ku.tiles_x = kp.utiles_x;
@@ -821,32 +823,38 @@ static cudaError_t stencil_u_t(const void* Vin, void* Vout, const uint8_t* occ,
     const size_t smem = stencil_u_smem(kp.nctl);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_stencil_u<S, kURX, UStencilR<S>::R>,
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_u<S, kURX, R, ARGMIN>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    k_stencil_u<S, kURX, UStencilR<S>::R><<<(unsigned)blocks, kp.ublock, smem, st>>>(
-        (const S*)Vin, (S*)Vout, occ, mask, ku, ctl, order, sb.part_sum, sb.part_max, argmin);
+    k_stencil_u<S, kURX, R, ARGMIN><<<(unsigned)blocks, kp.ublock, smem, st>>>(
+        (const S*)Vin, (S*)Vout, occ, mask, recs, ku, order, sb.part_sum, sb.part_max, argmin);
     k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
     *launches += 2;
     return cudaGetLastError();
 }
 
 cudaError_t launch_stencil_u(int storage, const void* Vin, void* Vout, const uint8_t* occ,
-                             const uint32_t* mask, const KParams& kp, const float* ctl,
+                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                              const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                              cudaStream_t st, int64_t* launches) {
+#define PG_SU(S)                                                                                 \
+    return argmin ? stencil_u_t<S, true>(Vin, Vout, occ, mask, recs, kp, order, sb, argmin, st,  \
+                                         launches)                                               \
+                  : stencil_u_t<S, false>(Vin, Vout, occ, mask, recs, kp, order, sb, argmin, st, \
+                                          launches)
     switch (storage) {
-        case PG_STORE_F32:
-            return stencil_u_t<float>(Vin, Vout, occ, mask, kp, ctl, order, sb, argmin, st, launches);
-        case PG_STORE_F16:
-            return stencil_u_t<__half>(Vin, Vout, occ, mask, kp, ctl, order, sb, argmin, st, launches);
-        case PG_STORE_BF16:
-            return stencil_u_t<__nv_bfloat16>(Vin, Vout, occ, mask, kp, ctl, order, sb, argmin, st,
-                                              launches);
+        case PG_STORE_F32: PG_SU(float);
+        case PG_STORE_F16: PG_SU(__half);
+        case PG_STORE_BF16: PG_SU(__nv_bfloat16);
     }
+#undef PG_SU
     return cudaErrorInvalidValue;
+}
+
+size_t stencil_recs_bytes(const KParams& kp) {
+    return (size_t)kp.nplanes * kp.nctl * kURec * sizeof(uint32_t);
 }
 
 size_t stencil_mask_bytes(const KParams& kp) {

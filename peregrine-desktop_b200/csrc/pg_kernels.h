@@ -33,12 +33,14 @@ cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t
                           double scale, double escape_scale, int64_t lo, int64_t n, uint8_t* out,
                           unsigned long long* counts, cudaStream_t st);
 
-cudaError_t launch_stencil_mask(const uint8_t* occ, const KParams& kp, const float* ctl,
-                                uint32_t* mask, cudaStream_t st, int64_t* launches);
+cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const float* ctl,
+                                uint32_t* mask, uint32_t* recs, cudaStream_t st,
+                                int64_t* launches);
 cudaError_t launch_stencil_u(int storage, const void* Vin, void* Vout, const uint8_t* occ,
-                             const uint32_t* mask, const KParams& kp, const float* ctl,
+                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                              const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                              cudaStream_t st, int64_t* launches);
+size_t stencil_recs_bytes(const KParams& kp);
 size_t stencil_mask_bytes(const KParams& kp);
 
 int64_t cellform_blocks(int64_t ncells);
