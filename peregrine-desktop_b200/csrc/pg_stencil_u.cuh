@@ -28,7 +28,9 @@ __host__ __device__ inline int32_t mask_words(int32_t n2) { return (n2 + 31) / 3
 
 // Record per (plane, control), 56 words, 16-byte aligned:
 //   float: wa[16] = w_hv*(1-tx), wb[16] = w_hv*tx, tau, ty, -, -
-//   int:   plane[16], ok, ox, oy, -
+//   int:   plane[16], ox, oy, ok, -   (every vector load on a record is
+//          aligned to its size: the record is 224 bytes, (tau, ty) sits at
+//          byte 128 and (ox, oy) at byte 208)
 constexpr int kUNT = 36;
 constexpr int kUNI = 20;
 constexpr int kURec = kUNT + kUNI;
@@ -90,9 +92,9 @@ __global__ void __launch_bounds__(256)
         rec[33] = __float_as_uint(ty);
         rec[34] = 0u;
         rec[35] = 0u;
-        rec[kUNT + 16] = t.ok ? 1u : 0u;
-        rec[kUNT + 17] = (uint32_t)(t.ok ? (int32_t)fx : 0);
-        rec[kUNT + 18] = (uint32_t)(t.ok ? (int32_t)fy : 0);
+        rec[kUNT + 16] = (uint32_t)(t.ok ? (int32_t)fx : 0);
+        rec[kUNT + 17] = (uint32_t)(t.ok ? (int32_t)fy : 0);
+        rec[kUNT + 18] = t.ok ? 1u : 0u;
         rec[kUNT + 19] = 0u;
     }
     __syncthreads();
@@ -364,7 +366,8 @@ __global__ void __launch_bounds__(256, 2)
                 const float* rec = reinterpret_cast<const float*>(srec + (size_t)u * kURec);
                 const int32_t* irec = reinterpret_cast<const int32_t*>(srec + (size_t)u * kURec + kUNT);
                 const float2 tt = *reinterpret_cast<const float2*>(rec + 32);
-                const int2 oo = *reinterpret_cast<const int2*>(irec + 17);
+                // (ox, oy) at record word 52: 8-byte aligned for the int2 load
+                const int2 oo = *reinterpret_cast<const int2*>(irec + 16);
                 const float tau = tt.x, ty = tt.y;
                 const int32_t ox = oo.x, oy = oo.y;
                 int32_t roff[RX + 1];
