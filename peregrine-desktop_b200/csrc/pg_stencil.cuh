@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(256)
                 continue;
             }
             if (argmin) argmin[L.rowmajor(i1, j, i3, i4, i5, i6)] = (int16_t)bk[r];
-            if (best[r] < old[r] || (kp.relax && best[r] != old[r])) {
+            if (best[r] < old[r] || (kp.relax && old[r] > (T)0 && best[r] != old[r])) {
                 const S nv = Conv<S>::template st<T>(best[r]);
                 const T nvT = (T)Conv<S>::val(nv);
                 Vout[didx] = nv;

@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(256, 2)
                 const bool lv = (live >> (a * R + r)) & 1u;
                 if constexpr (ARGMIN)
                     argmin[L.rowmajor(i, j, pq6[0], pq6[1], pq6[2], pq6[3])] = lv ? (int16_t)bk[a][r] : (int16_t)-1;
-                if (lv && (best[a][r] < old || (kp.relax && best[a][r] != old))) {
+                if (lv && (best[a][r] < old || (kp.relax && old > 0.0f && best[a][r] != old))) {
                     const S nv = Conv<S>::template st<float>(best[a][r]);
                     const float nvT = (float)Conv<S>::val(nv);
                     Vout[didx] = nv;

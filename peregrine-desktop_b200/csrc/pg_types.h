@@ -31,7 +31,8 @@ struct KParams {
     int32_t utile_x;  // masked stencil: x rows per block
     int32_t utiles_x; // masked stencil: blocks per plane
     int32_t ublock;   // masked stencil: threads per block
-    int32_t relax;    // 0: V' = min(V, T V), the reference's update; 1: V' = T V
+    int32_t relax;    // 0: V' = min(V, T V), the reference's update; 1: V' = T V except
+                      // where V = 0 (target cells, which stay pinned)
     int32_t phase;
 };
 
