@@ -212,6 +212,35 @@ int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
 /* Number of this library's kernel launches since the context was created. */
 int pg_launch_count(pg_ctx* ctx, int64_t* launches);
 
+/* One Jacobi sweep that allocates nothing.  No counterpart in the reference:
+ * it is for callers that cannot call cudaMalloc (a host that owns all device
+ * memory through its own pool or a fixed budget, or code that must not
+ * allocate after start-up), which the staged calls above cannot serve
+ * because they allocate their own buffers.
+ *
+ * Runs the cell-form sweep (the scheme pg_sweep runs with
+ * PG_KERNEL_CELLFORM on FP32 storage, phase as there) on device buffers the
+ * caller holds, on the current CUDA device and on `stream` (NULL: the
+ * default stream), and waits for it to finish:
+ *   v_in_dev, v_out_dev  float[ncells], different buffers, plane-major:
+ *                        index (((ih*Nvx+ivx)*Nvy+ivy)*Nw+iw)*Nx*Ny + ix*Ny + iy
+ *   occ_dev              uint8[Nh*Nx*Ny], index (ih*Nx+ix)*Ny+iy, nonzero = occupied
+ *   ctl_dev              float[3*nctl], the u1 column, then u2, then u3
+ * delta / maxnorm (may be NULL) receive the sweep's L1 and max decrease.
+ *
+ * Its only working memory is a 1 MiB array compiled into the library, which
+ * every GPU that loads the library holds until the process exits; grids of
+ * more than 8,388,608 cells are refused with PG_EINVAL.  Every call shares
+ * the array and it keeps the last call's contents: each call clears or
+ * writes every slot it reads, and calls that overlap on the GPU race on it.
+ * The first call on a device looks up the array's device address (set-up,
+ * with that device current); make that first call before any stream capture.
+ * Calls no cudaMalloc, cudaFree or other allocating routine. */
+int pg_sweep_noalloc(const pg_grid6* g, const pg_model* m, const pg_params* p,
+                     const uint8_t* occ_dev, const float* ctl_dev, int32_t nctl,
+                     const float* v_in_dev, float* v_out_dev, int32_t phase,
+                     void* stream, double* delta, double* maxnorm);
+
 #ifdef __cplusplus
 }
 #endif

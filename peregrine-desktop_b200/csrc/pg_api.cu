@@ -273,6 +273,10 @@ int iterate(pg_ctx* ctx, int kernel, bool esc, int32_t iters, double tol, int st
 
 }  // namespace
 
+namespace pg {
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace pg
+
 extern "C" {
 
 int32_t pg_abi_version(void) { return PG_ABI_VERSION; }

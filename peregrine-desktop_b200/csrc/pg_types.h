@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 
 #include "peregrine_hjb.h"
 
@@ -44,5 +45,8 @@ struct SweepBufs {
     int64_t nparts;
     double* out;  // [2]: L1 total, max-norm
 };
+
+// Records msg as the text pg_last_error returns on this thread; returns code.
+int set_last_error(int code, const std::string& msg);
 
 }  // namespace pg

@@ -31,7 +31,7 @@ EXPORTS = (
     "pg_abi_version", "pg_last_error", "pg_default_opts", "pg_create", "pg_destroy",
     "pg_solve_value", "pg_load_problem", "pg_solve", "pg_get_value", "pg_set_value",
     "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
-    "pg_launch_count",
+    "pg_launch_count", "pg_sweep_noalloc",
 )
 
 
@@ -113,6 +113,8 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "pg_encode": (C.c_int, [vp, i32, f64, f64, i64, i64, vp, P(i64), P(i64)]),
         "pg_time_sweeps": (C.c_int, [vp, i32, i32, i32, P(f64)]),
         "pg_launch_count": (C.c_int, [vp, P(i64)]),
+        "pg_sweep_noalloc": (C.c_int, [P(Grid6), P(Model), P(Params), vp, vp, i32, vp, vp, i32,
+                                       vp, P(f64), P(f64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -251,6 +253,27 @@ class Context:
         n = C.c_int64()
         _check(self._lib.pg_launch_count(self._h, C.byref(n)))
         return n.value
+
+
+def sweep_noalloc(grid: Grid6, model: Model, params: Params, occ_dev: int, ctl_dev: int,
+                  nctl: int, v_in_dev: int, v_out_dev: int, phase: int = 0,
+                  stream: int = 0) -> tuple[float, float]:
+    """One cell-form sweep on device buffers the caller owns, allocating nothing.
+
+    For callers that cannot allocate device memory themselves (their own pool
+    or a fixed budget owns the device).  The arguments are raw device
+    addresses (e.g. ``tensor.data_ptr()``) in the layouts pg_sweep_noalloc
+    documents: V plane-major, occupancy (h, x, y), controls as three columns.
+    Returns (L1 decrease, max decrease).  Grids above 8,388,608 cells are
+    refused.
+    """
+    lib = load_library()
+    d, dm = C.c_double(), C.c_double()
+    _check(lib.pg_sweep_noalloc(C.byref(grid), C.byref(model), C.byref(params),
+                                C.c_void_p(occ_dev), C.c_void_p(ctl_dev), int(nctl),
+                                C.c_void_p(v_in_dev), C.c_void_p(v_out_dev), int(phase),
+                                C.c_void_p(stream), C.byref(d), C.byref(dm)))
+    return d.value, dm.value
 
 
 def _wrap_cb(progress):
