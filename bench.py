@@ -35,7 +35,7 @@ for _p in (ROOT, PKG):
 METRIC = "Bellman cell-control updates/s; time-to-converge vs plain FP32 at ≤2 ms max err"
 UNIT = "cell-control updates/s"
 WORKLOAD = "medium"
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_stencil_medium_fp32.md")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_stencil_b_medium_fp32.md")
 
 
 def peaks():
@@ -44,6 +44,40 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def blend_tile_rows(n1: int, n2: int) -> int:
+    """Rows per block of the blend-then-shift sweep (the library's tiling:
+    whole rows, at most 1024 cells, as few tiles per plane as that allows)."""
+    tx = min(n1, 1024 // n2)
+    nt = -(-n1 // tx)
+    return -(-n1 // nt)
+
+
+def onchip_rooflines(pr, rate_per_gpu: float, elem: int, peaks_onchip) -> dict:
+    """The sweep's on-chip ceilings.  Per cell-control the blend-then-shift
+    kernel reads 16 corner-plane elements per window value ((TX+3)/TX window
+    values per cell) through L1, writes the window to shared memory as FP32
+    and reads 4 of its values back; it spends 16 (TX+3)/TX + 3 FMAs plus an
+    add and two mins."""
+    n1, n2 = int(pr.grid.n[0]), int(pr.grid.n[1])
+    tx = blend_tile_rows(n1, n2)
+    win = (tx + 3) / tx
+    bytes_cc = 16 * elem * win + 4 * win + 16
+    flops_cc = 2 * (16 * win + 3) + 3
+    out = {"tile_rows": tx, "bytes_per_update": bytes_cc, "flops_per_update": flops_cc}
+    if peaks_onchip:
+        g = rate_per_gpu * bytes_cc / 1e9
+        f = rate_per_gpu * flops_cc / 1e12
+        out["gather"] = {"achieved": g, "peak": peaks_onchip["smem_gbs"], "unit": "GB/s",
+                         "frac": g / peaks_onchip["smem_gbs"],
+                         "peak_source": "measured on this GPU (pg_measure_peaks, shared-memory "
+                                        "read bandwidth)"}
+        out["fma"] = {"achieved": f, "peak": peaks_onchip["fma_tflops"], "unit": "TFLOP/s",
+                      "frac": f / peaks_onchip["fma_tflops"],
+                      "peak_source": "measured on this GPU (pg_measure_peaks, FP32 FMA)"}
+        out["l2_read_gbs_measured"] = peaks_onchip["l2_gbs"]
+    return out
 
 
 def profiled_traffic():
@@ -152,7 +186,7 @@ def workload_config(pr, extra=None):
         "controls": pr.nctl,
         "step": "one Jacobi sweep over every cell and control",
         "l2": "inputs larger than L2 (V is 0.995 GB per buffer, two buffers)",
-        "kernel": "k_stencil<float,float,FMA>",
+        "kernel": "k_stencil_b<float> (blend-then-shift)",
     }
     if extra:
         cfg.update(extra)
@@ -278,6 +312,12 @@ def run_ours(args, rank, world, local_rank):
     alg_bytes = 2 * 4 * pr.ncells  # read V once + write V once per sweep
     achieved = alg_bytes / (ms / 1000.0) / 1e9
     traffic = profiled_traffic()
+    try:
+        pk = _lib.measure_peaks(local_rank)
+    except Exception as exc:  # the line still reports the HBM roofline
+        print(f"peak probes failed: {exc}", file=sys.stderr)
+        pk = None
+    onchip = onchip_rooflines(pr, cc_per_sweep / (ms / 1000.0), 4, pk)
 
     # ---- CPU baseline: the oracle on the host cores, bounded sample
     from oracle import oracle as og
@@ -293,7 +333,10 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "algorithmic_bytes_per_launch": alg_bytes},
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "timed": "CUDA events around the sweep launches on the context stream "
+                              "(sweep kernel + its one-block residual reduction)",
+                     "onchip": onchip},
         "cpu_baseline": {"value": cpu_rate, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{n_cpu} contiguous cells x {pr.nctl} controls, one Jacobi "
                                    f"pass ({dt_cpu:.1f} s) of the same workload"},

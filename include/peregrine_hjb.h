@@ -102,6 +102,7 @@ typedef struct pg_params {
 #define PG_KERNEL_CELLFORM 2  /* one thread per cell, the full cell_update     */
 #define PG_KERNEL_STENCIL_EXACT 3 /* stencil with the reference's rounding order */
 #define PG_KERNEL_STENCIL_ROWS  4 /* stencil deciding every probe per sweep (no mask) */
+#define PG_KERNEL_STENCIL_GATHER 5 /* masked stencil gathering all 64 corners per cell */
 
 /* Table dtypes (solver/src/Pipeline.jl:620-625). */
 #define PG_DTYPE_U8  0
@@ -211,6 +212,14 @@ int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
 
 /* Number of this library's kernel launches since the context was created. */
 int pg_launch_count(pg_ctx* ctx, int64_t* launches);
+
+/* On-chip ceilings of `device`, measured: shared-memory read bandwidth
+ * (GB/s, all SMs), read bandwidth of an L2-resident 64 MiB buffer (GB/s) and
+ * FP32 FMA throughput (TFLOP/s).  No counterpart in the reference: the
+ * secondary rooflines of the sweep (on-chip bytes and FMAs per lookahead) are
+ * quoted against these.  Any output may be NULL to skip that probe. */
+int pg_measure_peaks(int device, double* smem_gbs, double* l2_gbs,
+                     double* fma_tflops);
 
 /* One Jacobi sweep that allocates nothing.  No counterpart in the reference:
  * it is for callers that cannot call cudaMalloc (a host that owns all device

@@ -81,6 +81,8 @@ struct pg_ctx {
     uint32_t* mask_d = nullptr;  // admissibility bits of the masked stencil
     uint32_t* recs_d = nullptr;  // its per-(plane, control) records
     bool mask_ok = false;
+    bool blend_ok = false;   // the blend-then-shift tiling fits (shared memory, row width)
+    bool gather_ok = false;  // the 64-corner masked gather fits its shared memory
     int8_t* pol_d = nullptr;
     double* part_sum = nullptr;
     double* part_max = nullptr;
@@ -114,6 +116,8 @@ struct pg_ctx {
         if (recs_d) cudaFree(recs_d);
         recs_d = nullptr;
         mask_ok = false;
+        blend_ok = false;
+        gather_ok = false;
         if (pol_d) cudaFree(pol_d);
         if (part_sum) cudaFree(part_sum);
         if (part_max) cudaFree(part_max);
@@ -175,7 +179,9 @@ int pick_kernel(pg_ctx* ctx, int32_t kernel, int* out) {
         return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
     if (kernel == PG_KERNEL_STENCIL_ROWS && !ctx->stencil_ok)
         return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
-    if (kernel < PG_KERNEL_STENCIL || kernel > PG_KERNEL_STENCIL_ROWS)
+    if (kernel == PG_KERNEL_STENCIL_GATHER && !ctx->stencil_ok)
+        return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
+    if (kernel < PG_KERNEL_STENCIL || kernel > PG_KERNEL_STENCIL_GATHER)
         return fail(PG_EINVAL, "unknown kernel " + std::to_string(kernel));
     *out = kernel;
     return PG_OK;
@@ -193,7 +199,13 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
         e = pg::launch_cellform(ctx->storage, esc, vin, vout, ctx->occ_d,
                                 use_pol ? ctx->pol_d : nullptr, ctx->kp, ctx->ctl_d, sb, argmin_d,
                                 ctx->stream, &ctx->launches);
-    else if (kernel == PG_KERNEL_STENCIL && ctx->mask_ok && ctx->storage != PG_STORE_F64)
+    else if (kernel == PG_KERNEL_STENCIL && ctx->mask_ok && ctx->blend_ok &&
+             ctx->storage != PG_STORE_F64)
+        e = pg::launch_stencil_b(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
+                                 ctx->kp, ctx->order_d, sb, argmin_d, ctx->stream,
+                                 &ctx->launches);
+    else if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_GATHER) && ctx->mask_ok &&
+             ctx->gather_ok && ctx->storage != PG_STORE_F64)
         e = pg::launch_stencil_u(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  ctx->kp, ctx->order_d, sb, argmin_d, ctx->stream,
                                  &ctx->launches);
@@ -404,6 +416,19 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
         }
         kp.ublock = best_bs;
     }
+    // Blend-then-shift: a block takes whole rows of one plane, at most
+    // 1024 cells (4 per thread), as few tiles per plane as that allows.
+    if (g->n[1] <= pg::kBMaxTileCells) {
+        int32_t tx = std::min<int32_t>(g->n[0], pg::kBMaxTileCells / g->n[1]);
+        const int32_t nt = (g->n[0] + tx - 1) / tx;
+        tx = (g->n[0] + nt - 1) / nt;
+        const int64_t cells = (int64_t)tx * g->n[1];
+        int64_t th = 32 * (((cells + 2) / 3 + 31) / 32);
+        th = std::max<int64_t>(64, std::min<int64_t>(256, th));
+        kp.btile_x = tx;
+        kp.btiles_x = nt;
+        kp.bblock = (int32_t)th;
+    }
     kp.nsub = host_substeps_for(p->cfl <= 0.0f ? p->dt : p->tau_max, *p);
     kp.nchk = p->checks;
 
@@ -462,6 +487,8 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     if (sb > ctx->nparts) ctx->nparts = sb;
     const int64_t ub = kp.nplanes * kp.utiles_x;
     if (ub > ctx->nparts) ctx->nparts = ub;
+    const int64_t bb = kp.nplanes * kp.btiles_x;
+    if (bb > ctx->nparts) ctx->nparts = bb;
     PG_CUDA(cudaMalloc(&ctx->part_sum, sizeof(double) * ctx->nparts));
     PG_CUDA(cudaMalloc(&ctx->part_max, sizeof(double) * ctx->nparts));
     // The admissibility mask of the masked stencil: decided once here, read by
@@ -477,6 +504,8 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
                                                     ctx->recs_d, ctx->stream, &ctx->launches);
             if (e != cudaSuccess) return fail(PG_ECUDA, std::string("prep: ") + cudaGetErrorString(e));
             ctx->mask_ok = true;
+            ctx->blend_ok = kp.btile_x > 0 && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
+            ctx->gather_ok = pg::stencil_u_smem_bytes(kp) <= 200 * 1024;
         } else {
             cudaGetLastError();
             if (ctx->mask_d) cudaFree(ctx->mask_d);

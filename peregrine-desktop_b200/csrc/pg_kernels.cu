@@ -553,6 +553,7 @@ __global__ void __launch_bounds__(kCellThreads)
 #include "pg_plane.cuh"
 #include "pg_stencil.cuh"
 #include "pg_stencil_u.cuh"
+#include "pg_stencil_b.cuh"
 
 // ---------------------------------------------------------------------------
 // Encoding (encode_into!, Pipeline.jl:698-780), from the device layout into
@@ -852,6 +853,70 @@ cudaError_t launch_stencil_u(int storage, const void* Vin, void* Vout, const uin
 #undef PG_SU
     return cudaErrorInvalidValue;
 }
+
+template <typename S, bool ARGMIN, bool VEC>
+static cudaError_t stencil_b_v(const void* Vin, void* Vout, const uint8_t* occ,
+                               const uint32_t* mask, const uint32_t* recs, const KParams& kb,
+                               const int32_t* order, const SweepBufs& sb, int16_t* argmin,
+                               int64_t blocks, int threads, size_t smem, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_b<S, ARGMIN, VEC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_stencil_b<S, ARGMIN, VEC><<<(unsigned)blocks, threads, smem, st>>>(
+        (const S*)Vin, (S*)Vout, occ, mask, recs, kb, order, sb.part_sum, sb.part_max, argmin);
+    return cudaSuccess;
+}
+
+template <typename S, bool ARGMIN>
+static cudaError_t stencil_b_t(const void* Vin, void* Vout, const uint8_t* occ,
+                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                               const int32_t* order, const SweepBufs& sb, int16_t* argmin,
+                               cudaStream_t st, int64_t* launches) {
+    if (kp.btile_x <= 0 || kp.bblock <= 0 || kp.bblock > 256 || kp.nsub > kStencilMaxSub ||
+        (int64_t)kp.btile_x * kp.g.n[1] > (int64_t)kp.bblock * kBCells)
+        return cudaErrorInvalidValue;
+    KParams kb = kp;
+    kb.tile_x = kp.btile_x;
+    kb.tiles_x = kp.btiles_x;
+    const int64_t blocks = kp.nplanes * kp.btiles_x;
+    if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const size_t smem = stencil_b_smem(kp.btile_x, kp.g.n[1]);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    const bool vec = kp.g.n[1] % BVec<S>::N == 0;
+    cudaError_t e = vec ? stencil_b_v<S, ARGMIN, true>(Vin, Vout, occ, mask, recs, kb, order, sb,
+                                                        argmin, blocks, kp.bblock, smem, st)
+                        : stencil_b_v<S, ARGMIN, false>(Vin, Vout, occ, mask, recs, kb, order, sb,
+                                                         argmin, blocks, kp.bblock, smem, st);
+    if (e != cudaSuccess) return e;
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uint8_t* occ,
+                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                             const int32_t* order, const SweepBufs& sb, int16_t* argmin,
+                             cudaStream_t st, int64_t* launches) {
+#define PG_SB(S)                                                                                 \
+    return argmin ? stencil_b_t<S, true>(Vin, Vout, occ, mask, recs, kp, order, sb, argmin, st,  \
+                                         launches)                                               \
+                  : stencil_b_t<S, false>(Vin, Vout, occ, mask, recs, kp, order, sb, argmin, st, \
+                                          launches)
+    switch (storage) {
+        case PG_STORE_F32: PG_SB(float);
+        case PG_STORE_F16: PG_SB(__half);
+        case PG_STORE_BF16: PG_SB(__nv_bfloat16);
+    }
+#undef PG_SB
+    return cudaErrorInvalidValue;
+}
+
+size_t stencil_b_smem_bytes(const KParams& kp) { return stencil_b_smem(kp.btile_x, kp.g.n[1]); }
+size_t stencil_u_smem_bytes(const KParams& kp) { return stencil_u_smem(kp.nctl); }
 
 size_t stencil_recs_bytes(const KParams& kp) {
     return (size_t)kp.nplanes * kp.nctl * kURec * sizeof(uint32_t);

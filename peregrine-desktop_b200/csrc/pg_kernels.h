@@ -40,6 +40,12 @@ cudaError_t launch_stencil_u(int storage, const void* Vin, void* Vout, const uin
                              const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                              const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                              cudaStream_t st, int64_t* launches);
+cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uint8_t* occ,
+                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                             const int32_t* order, const SweepBufs& sb, int16_t* argmin,
+                             cudaStream_t st, int64_t* launches);
+size_t stencil_b_smem_bytes(const KParams& kp);
+size_t stencil_u_smem_bytes(const KParams& kp);
 size_t stencil_recs_bytes(const KParams& kp);
 size_t stencil_mask_bytes(const KParams& kp);
 

@@ -26,14 +26,17 @@ constexpr int kURX = 2;  // rows per thread
 // Mask words per (plane, control, row): ceil(Ny / 32).
 __host__ __device__ inline int32_t mask_words(int32_t n2) { return (n2 + 31) / 32; }
 
-// Record per (plane, control), 56 words, 16-byte aligned:
-//   float: wa[16] = w_hv*(1-tx), wb[16] = w_hv*tx, tau, ty, -, -
-//   int:   plane[16], ox, oy, ok, -   (every vector load on a record is
-//          aligned to its size: the record is 224 bytes, (tau, ty) sits at
-//          byte 128 and (ox, oy) at byte 208)
-constexpr int kUNT = 36;
+// Record per (plane, control), 72 words, 16-byte aligned:
+//   float: w[16] (the (h, v)-corner weights), tau, tx, ty, -
+//   int:   plane[16], ox, oy, ok, nsub
+//   float: incx[16], incy[16] (the field-frame position increment of each
+//          substep, which the reference adds to x and y one at a time)
+// Every vector load on a record is aligned to its size: the record is 288
+// bytes, (tau, tx, ty, -) sits at byte 64 and (ox, oy) at byte 144.
+constexpr int kUNT = 20;
 constexpr int kUNI = 20;
-constexpr int kURec = kUNT + kUNI;
+constexpr int kUInc = 40;
+constexpr int kURec = kUInc + 2 * kStencilMaxSub;
 
 __host__ __device__ inline size_t stencil_u_smem(int nctl) {
     return (size_t)nctl * (kURec * 4 + 4) + 64;
@@ -83,19 +86,21 @@ __global__ void __launch_bounds__(256)
         const float fx = floorf(dxc), fy = floorf(dyc);
         const float tx = dxc - fx, ty = dyc - fy;
         for (int c = 0; c < 16; ++c) {
-            const float w = corner_weight(t, c);
-            rec[c] = __float_as_uint(w * (1.0f - tx));
-            rec[16 + c] = __float_as_uint(w * tx);
+            rec[c] = __float_as_uint(corner_weight(t, c));
             rec[kUNT + c] = (uint32_t)corner_plane(g, t, c);
         }
-        rec[32] = __float_as_uint(t.tau);
-        rec[33] = __float_as_uint(ty);
-        rec[34] = 0u;
-        rec[35] = 0u;
+        rec[16] = __float_as_uint(t.tau);
+        rec[17] = __float_as_uint(tx);
+        rec[18] = __float_as_uint(ty);
+        rec[19] = 0u;
         rec[kUNT + 16] = (uint32_t)(t.ok ? (int32_t)fx : 0);
         rec[kUNT + 17] = (uint32_t)(t.ok ? (int32_t)fy : 0);
         rec[kUNT + 18] = t.ok ? 1u : 0u;
-        rec[kUNT + 19] = 0u;
+        rec[kUNT + 19] = (uint32_t)nsub;
+        for (int k = 0; k < kStencilMaxSub; ++k) {
+            rec[kUInc + k] = __float_as_uint(t.ok && k < nsub ? t.incx[k] : 0.0f);
+            rec[kUInc + kStencilMaxSub + k] = __float_as_uint(t.ok && k < nsub ? t.incy[k] : 0.0f);
+        }
     }
     __syncthreads();
     const int32_t n1 = L.n[0], n2 = L.n[1], W = mask_words(n2);
@@ -203,7 +208,7 @@ __host__ __device__ constexpr int span_index(int k) {
 // a (0..RX-1, already combined with row a+1 along x) and columns k (0..R).
 template <typename S, int RX, int R, int MODE, int PARAM>
 __device__ __forceinline__ void gather_vec(const S* __restrict__ Vin, int64_t P,
-                                           const int32_t* irec, const float* rec,
+                                           const int32_t* irec, const float* rec, float tx,
                                            const int32_t* roff, int32_t c0,
                                            float (&m)[RX][R + 1]) {
     constexpr int VEC = VecElem<S>::VEC;
@@ -211,7 +216,7 @@ __device__ __forceinline__ void gather_vec(const S* __restrict__ Vin, int64_t P,
 #pragma unroll 2
     for (int c = 0; c < 16; ++c) {
         const int32_t pq = irec[c];
-        const float wa = rec[c], wb = rec[16 + c];
+        const float wa = rec[c] * (1.0f - tx), wb = rec[c] * tx;
         const S* Vc = Vin + (int64_t)pq * P + c0;
         float v[RX + 1][R + 1];
 #pragma unroll
@@ -239,13 +244,13 @@ __device__ __forceinline__ void gather_vec(const S* __restrict__ Vin, int64_t P,
 // Any columns (clamped to the row), one load per value.
 template <typename S, int RX, int R>
 __device__ __forceinline__ void gather_scalar(const S* __restrict__ Vin, int64_t P,
-                                              const int32_t* irec, const float* rec,
+                                              const int32_t* irec, const float* rec, float tx,
                                               const int32_t* roff, const int32_t* coff,
                                               float (&m)[RX][R + 1]) {
 #pragma unroll 2
     for (int c = 0; c < 16; ++c) {
         const int32_t pq = irec[c];
-        const float wa = rec[c], wb = rec[16 + c];
+        const float wa = rec[c] * (1.0f - tx), wb = rec[c] * tx;
         const S* Vc = Vin + (int64_t)pq * P;
         float v[RX + 1][R + 1];
 #pragma unroll
@@ -365,10 +370,10 @@ __global__ void __launch_bounds__(256, 2)
                 }
                 const float* rec = reinterpret_cast<const float*>(srec + (size_t)u * kURec);
                 const int32_t* irec = reinterpret_cast<const int32_t*>(srec + (size_t)u * kURec + kUNT);
-                const float2 tt = *reinterpret_cast<const float2*>(rec + 32);
-                // (ox, oy) at record word 52: 8-byte aligned for the int2 load
+                const float4 tt = *reinterpret_cast<const float4*>(rec + 16);
+                // (ox, oy) at record word 36: 8-byte aligned for the int2 load
                 const int2 oo = *reinterpret_cast<const int2*>(irec + 16);
-                const float tau = tt.x, ty = tt.y;
+                const float tau = tt.x, tx = tt.y, ty = tt.z;
                 const int32_t ox = oo.x, oy = oo.y;
                 int32_t roff[RX + 1];
 #pragma unroll
@@ -384,7 +389,7 @@ __global__ void __launch_bounds__(256, 2)
                     const int mis = oy & (VEC - 1);
                     const int32_t c0 = j0 + oy - mis;
                     switch (mis) {
-#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 0, MM>(Vin, P, irec, rec, roff, c0, m); break;
+#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 0, MM>(Vin, P, irec, rec, tx, roff, c0, m); break;
                         PG_GV(0) PG_GV(1) PG_GV(2) PG_GV(3) PG_GV(4) PG_GV(5) PG_GV(6) PG_GV(7)
 #undef PG_GV
                     }
@@ -392,13 +397,13 @@ __global__ void __launch_bounds__(256, 2)
                     if (oy >= 0) {
                         const int mis = oy & (VEC - 1);
                         switch (mis) {
-#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 0, MM>(Vin, P, irec, rec, roff, oy - MM, m); break;
+#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 0, MM>(Vin, P, irec, rec, tx, roff, oy - MM, m); break;
                             PG_GV(0) PG_GV(1) PG_GV(2) PG_GV(3) PG_GV(4) PG_GV(5) PG_GV(6) PG_GV(7)
 #undef PG_GV
                         }
                     } else {
                         switch (-oy) {
-#define PG_GV(MM) case MM: if constexpr (MM >= 1 && MM <= VEC) gather_vec<S, RX, R, 1, MM>(Vin, P, irec, rec, roff, 0, m); break;
+#define PG_GV(MM) case MM: if constexpr (MM >= 1 && MM <= VEC) gather_vec<S, RX, R, 1, MM>(Vin, P, irec, rec, tx, roff, 0, m); break;
                             PG_GV(1) PG_GV(2) PG_GV(3) PG_GV(4) PG_GV(5) PG_GV(6) PG_GV(7) PG_GV(8)
 #undef PG_GV
                         }
@@ -407,13 +412,13 @@ __global__ void __launch_bounds__(256, 2)
                     if (oy < 0) {
                         const int mis = oy & (VEC - 1);
                         switch (mis) {
-#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 0, MM>(Vin, P, irec, rec, roff, j0 + oy - MM, m); break;
+#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 0, MM>(Vin, P, irec, rec, tx, roff, j0 + oy - MM, m); break;
                             PG_GV(0) PG_GV(1) PG_GV(2) PG_GV(3) PG_GV(4) PG_GV(5) PG_GV(6) PG_GV(7)
 #undef PG_GV
                         }
                     } else {
                         switch (oy) {
-#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 2, MM>(Vin, P, irec, rec, roff, n2 - NV * VEC, m); break;
+#define PG_GV(MM) case MM: if constexpr (MM < VEC) gather_vec<S, RX, R, 2, MM>(Vin, P, irec, rec, tx, roff, n2 - NV * VEC, m); break;
                             PG_GV(0) PG_GV(1) PG_GV(2) PG_GV(3) PG_GV(4) PG_GV(5) PG_GV(6) PG_GV(7)
 #undef PG_GV
                         }
@@ -422,7 +427,7 @@ __global__ void __launch_bounds__(256, 2)
                     int32_t coff[R + 1];
 #pragma unroll
                     for (int k = 0; k <= R; ++k) coff[k] = min(max(j0 + k + oy, 0), n2 - 1);
-                    gather_scalar<S, RX, R>(Vin, P, irec, rec, roff, coff, m);
+                    gather_scalar<S, RX, R>(Vin, P, irec, rec, tx, roff, coff, m);
                 }
 #pragma unroll
                 for (int a = 0; a < RX; ++a)

@@ -14,6 +14,9 @@ constexpr int kStencilMaxSub = 16;
 constexpr int kStencilMaxChk = 4;
 constexpr int kStencilThreads = 256;
 constexpr int kCellThreads = 128;
+// Blend-then-shift sweep: cells per thread, cells per block at most.
+constexpr int kBCells = 4;
+constexpr int kBMaxTileCells = 1024;
 
 // Everything a sweep kernel needs besides the arrays, passed by value.
 struct KParams {
@@ -32,6 +35,9 @@ struct KParams {
     int32_t utile_x;  // masked stencil: x rows per block
     int32_t utiles_x; // masked stencil: blocks per plane
     int32_t ublock;   // masked stencil: threads per block
+    int32_t btile_x;  // blend-then-shift: x rows per block (0: not eligible)
+    int32_t btiles_x; // blend-then-shift: blocks per plane
+    int32_t bblock;   // blend-then-shift: threads per block
     int32_t relax;    // 0: V' = min(V, T V), the reference's update; 1: V' = T V except
                       // where V = 0 (target cells, which stay pinned)
     int32_t phase;

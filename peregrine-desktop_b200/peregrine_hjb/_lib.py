@@ -22,8 +22,8 @@ PG_EINVAL, PG_ECUDA, PG_ENOMEM, PG_ETIMEOUT, PG_ESTATE, PG_EUNSUPPORTED, PG_ECAN
 STOP_L1_QUIET, STOP_MAXNORM = 0, 1
 STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
 STORAGES = {"fp32": STORE_F32, "fp16": STORE_F16, "bf16": STORE_BF16, "fp64": STORE_F64}
-KERNEL_AUTO, KERNEL_STENCIL, KERNEL_CELLFORM, KERNEL_STENCIL_EXACT, KERNEL_STENCIL_ROWS = (
-    0, 1, 2, 3, 4)
+(KERNEL_AUTO, KERNEL_STENCIL, KERNEL_CELLFORM, KERNEL_STENCIL_EXACT, KERNEL_STENCIL_ROWS,
+ KERNEL_STENCIL_GATHER) = (0, 1, 2, 3, 4, 5)
 DTYPE_CODES = {"u8": 0, "u16": 1, "f16": 2, "f32": 3}
 
 # Every symbol include/peregrine_hjb.h declares.
@@ -31,7 +31,7 @@ EXPORTS = (
     "pg_abi_version", "pg_last_error", "pg_default_opts", "pg_create", "pg_destroy",
     "pg_solve_value", "pg_load_problem", "pg_solve", "pg_get_value", "pg_set_value",
     "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
-    "pg_launch_count", "pg_sweep_noalloc",
+    "pg_launch_count", "pg_measure_peaks", "pg_sweep_noalloc",
 )
 
 
@@ -113,6 +113,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "pg_encode": (C.c_int, [vp, i32, f64, f64, i64, i64, vp, P(i64), P(i64)]),
         "pg_time_sweeps": (C.c_int, [vp, i32, i32, i32, P(f64)]),
         "pg_launch_count": (C.c_int, [vp, P(i64)]),
+        "pg_measure_peaks": (C.c_int, [C.c_int, P(f64), P(f64), P(f64)]),
         "pg_sweep_noalloc": (C.c_int, [P(Grid6), P(Model), P(Params), vp, vp, i32, vp, vp, i32,
                                        vp, P(f64), P(f64)]),
     }
@@ -253,6 +254,15 @@ class Context:
         n = C.c_int64()
         _check(self._lib.pg_launch_count(self._h, C.byref(n)))
         return n.value
+
+
+def measure_peaks(device: int = 0) -> dict:
+    """Shared-memory and L2 read bandwidth (GB/s) and FP32 FMA TFLOP/s of the
+    device, measured by the library's own probe kernels."""
+    lib = load_library()
+    s, l2, f = C.c_double(), C.c_double(), C.c_double()
+    _check(lib.pg_measure_peaks(int(device), C.byref(s), C.byref(l2), C.byref(f)))
+    return {"smem_gbs": s.value, "l2_gbs": l2.value, "fma_tflops": f.value}
 
 
 def sweep_noalloc(grid: Grid6, model: Model, params: Params, occ_dev: int, ctl_dev: int,
