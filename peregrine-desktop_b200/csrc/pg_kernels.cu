@@ -791,16 +791,20 @@ cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout,
 cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const float* ctl,
                                 uint32_t* mask, uint32_t* recs, cudaStream_t st,
                                 int64_t* launches) {
-    const size_t smem = stencil_prep_smem(kp.nctl, kp.nsub);
+    size_t smem = stencil_prep_smem(kp.nctl, kp.nsub);
+    const size_t tab = stencil_prep_tab_smem(kp.nctl, kp.g.n[1]);
+    const int coltab = kp.g.n[1] <= 255 && kp.nchk <= 4 && smem + tab <= 200 * 1024;
+    if (coltab) smem += tab;
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_prep,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     if (kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
-    k_stencil_prep<<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask, recs);
+    k_stencil_prep<<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask, recs, coltab);
     *launches += 1;
     return cudaGetLastError();
 }
@@ -884,7 +888,7 @@ static cudaError_t stencil_b_t(const void* Vin, void* Vout, const uint8_t* occ,
     kb.tiles_x = kp.btiles_x;
     const int64_t blocks = kp.nplanes * kp.btiles_x;
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-    const size_t smem = stencil_b_smem(kp.btile_x, kp.g.n[1]);
+    const size_t smem = stencil_b_smem(kp.nctl, kp.btile_x, kp.g.n[1]);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     const bool vec = kp.g.n[1] % BVec<S>::N == 0;
     cudaError_t e = vec ? stencil_b_v<S, ARGMIN, true>(Vin, Vout, occ, mask, recs, kb, order, sb,
@@ -915,7 +919,9 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
     return cudaErrorInvalidValue;
 }
 
-size_t stencil_b_smem_bytes(const KParams& kp) { return stencil_b_smem(kp.btile_x, kp.g.n[1]); }
+size_t stencil_b_smem_bytes(const KParams& kp) {
+    return stencil_b_smem(kp.nctl, kp.btile_x, kp.g.n[1]);
+}
 size_t stencil_u_smem_bytes(const KParams& kp) { return stencil_u_smem(kp.nctl); }
 
 size_t stencil_recs_bytes(const KParams& kp) {

@@ -29,10 +29,10 @@
 // reads instead of 64 shifted gathers.  FP32 arithmetic with FMAs; the
 // result differs from the reference's by the rounding order of the
 // interpolation sum, never in a corner, a fraction or an admissibility
-// decision (those are the mask's).  The per-(plane, control) records are
-// read straight from global memory: every lane of a warp reads the same
-// words, so they cost one L1 access per warp and leave shared memory (and
-// with it L1 capacity) to the windows.
+// decision (those are the mask's).  Each control's 288-byte record is
+// copied into shared memory with cp.async one control ahead, so its latency
+// hides behind the previous control's work and the block's shared memory
+// (and with it the L1 capacity left for the corner planes) stays small.
 
 // Elements of S in one 16-byte load.
 template <typename S> struct BVec { static constexpr int N = 16 / sizeof(S); };
@@ -68,11 +68,24 @@ template <> struct BUnpack<__nv_bfloat16> {
     }
 };
 
-// Shared memory of one block: two window buffers and two sets of per-row /
-// per-column successor corners.
-__host__ __device__ inline size_t stencil_b_smem(int tile_x, int n2) {
-    return 2 * (size_t)(tile_x + 3) * n2 * sizeof(float) +
+// Shared memory of one block: two record slots, the control order, two
+// window buffers and two sets of per-row / per-column successor corners.
+__host__ __device__ inline size_t stencil_b_smem(int nctl, int tile_x, int n2) {
+    return 2 * (size_t)kURec * 4 + (size_t)((nctl + 3) & ~3) * 4 +
+           2 * (size_t)(tile_x + 3) * n2 * sizeof(float) +
            2 * (size_t)(tile_x + n2) * 2 * sizeof(int32_t);
+}
+
+// 16-byte global -> shared copy that completes asynchronously (cp.async).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Block = (plane, tile of kp.tile_x rows x all columns).  VEC: n2 is a
@@ -90,7 +103,9 @@ __global__ void __launch_bounds__(256)
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], W = mask_words(n2);
     const int32_t TX = kp.tile_x;
     const int64_t bsz = (int64_t)(TX + 3) * n2;
-    float* Bbuf = reinterpret_cast<float*>(smem_raw);
+    uint32_t* rslot = reinterpret_cast<uint32_t*>(smem_raw);  // [2][kURec]
+    int32_t* ord = reinterpret_cast<int32_t*>(rslot + 2 * kURec);
+    float* Bbuf = reinterpret_cast<float*>(ord + ((nctl + 3) & ~3));
     // per control: (window row, x fraction) of each tile row and (lower
     // column, y fraction) of each column, double-buffered like the window
     int2* rinfo = reinterpret_cast<int2*>(Bbuf + 2 * bsz);
@@ -135,13 +150,27 @@ __global__ void __launch_bounds__(256)
         if (e < ncell && occ_h[e] == 0) live |= 1u << q;
     }
     const uint32_t* mplane = mask + ((size_t)pl * nctl * n1 + x0) * W;
+    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(order + i);
+    __syncthreads();
+    constexpr int kRecVec = kURec / 4;  // 16-byte pieces of a record
+    if (tid < kRecVec)
+        cp_async16(rslot + 4 * tid, prec + (size_t)ord[0] * kURec + 4 * tid);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
 
     int buf = 0;
     for (int uu = 0; uu < nctl; ++uu) {
-        const int u = __ldg(order + uu);
-        const uint32_t* rec = prec + (size_t)u * kURec;
+        const int u = ord[uu];
+        const uint32_t* rec = rslot + (uu & 1) * kURec;
+        // prefetch the next control's record into the other slot; it is
+        // waited for at this control's barrier
+        if (uu + 1 < nctl && tid < kRecVec)
+            cp_async16(rslot + ((uu + 1) & 1) * kURec + 4 * tid,
+                       prec + (size_t)ord[uu + 1] * kURec + 4 * tid);
+        cp_async_commit();
         // (ox, oy, ok, nsub)
-        const int4 oi = __ldg(reinterpret_cast<const int4*>(rec + kUNT + 16));
+        const int4 oi = *reinterpret_cast<const int4*>(rec + kUNT + 16);
         if (oi.z == 0) {
             // no cell of the plane admits this control (block-uniform)
             if constexpr (ARGMIN) {
@@ -149,8 +178,11 @@ __global__ void __launch_bounds__(256)
                 for (int q = 0; q < kBCells; ++q)
                     if (best[q] == cap && u < bk[q]) bk[q] = u;
             }
+            cp_async_wait_all();
+            __syncthreads();
             continue;
         }
+        const float tau = __uint_as_float(rec[16]);
         const int32_t wbase = x0 + oi.x - 1;
         float* B = Bbuf + buf * bsz;
         int2* ri = rinfo + buf * TX;
@@ -171,8 +203,8 @@ __global__ void __launch_bounds__(256)
                 for (int t = 0; t < VN; ++t) acc[t] = 0.0f;
 #pragma unroll 2
                 for (int c4 = 0; c4 < 4; ++c4) {
-                    const float4 w = __ldg(reinterpret_cast<const float4*>(rec) + c4);
-                    const int4 pq = __ldg(reinterpret_cast<const int4*>(rec + kUNT) + c4);
+                    const float4 w = reinterpret_cast<const float4*>(rec)[c4];
+                    const int4 pq = reinterpret_cast<const int4*>(rec + kUNT)[c4];
                     const uint4 q0 = __ldg(reinterpret_cast<const uint4*>(base + (int64_t)pq.x * P));
                     const uint4 q1 = __ldg(reinterpret_cast<const uint4*>(base + (int64_t)pq.y * P));
                     const uint4 q2 = __ldg(reinterpret_cast<const uint4*>(base + (int64_t)pq.z * P));
@@ -197,8 +229,8 @@ __global__ void __launch_bounds__(256)
                 float acc = 0.0f;
 #pragma unroll 4
                 for (int c = 0; c < 16; ++c) {
-                    const float w = __uint_as_float(__ldg(rec + c));
-                    const int32_t pc = (int32_t)__ldg(rec + kUNT + c);
+                    const float w = __uint_as_float(rec[c]);
+                    const int32_t pc = (int32_t)rec[kUNT + c];
                     acc = fmaf(w, (float)Conv<S>::ld(Vin + (int64_t)pc * P + off), acc);
                 }
                 B[it] = acc;
@@ -208,13 +240,15 @@ __global__ void __launch_bounds__(256)
         // per column, rounded as the reference rounds them
         for (int32_t it = tid; it < nr + n2; it += T) {
             const bool row = it < nr;
-            const int ax = row ? 0 : 1;
             const int32_t idx = row ? x0 + it : it - nr;
             const float* inc = reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
-            const float x = axisvalue(g, ax, idx);
+            // constant axis indices keep the grid in registers
+            const float x = row ? axisvalue(g, 0, idx) : axisvalue(g, 1, idx);
+            const float lo = row ? g.lo[0] : g.lo[1];
+            const float st = row ? g.step[0] : g.step[1];
             float xn = x;
-            for (int k = 0; k < oi.w; ++k) xn = R_::add(xn, __ldg(inc + k));
-            const float f = R_::div(R_::sub(xn, g.lo[ax]), g.step[ax]);
+            for (int k = 0; k < oi.w; ++k) xn = R_::add(xn, inc[k]);
+            const float f = R_::div(R_::sub(xn, lo), st);
             const float fl = floorf(f);
             const float t = R_::sub(f, fl);
             // successors off the table are never admissible; the clamps only
@@ -226,10 +260,11 @@ __global__ void __launch_bounds__(256)
             else
                 ci[it - nr] = make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
         }
+        cp_async_wait_all();
         __syncthreads();
 
-        // phase 2: shift, admissibility, tau, min
-        const float tau = __uint_as_float(__ldg(rec + 16));
+        // phase 2: shift, admissibility, tau, min (the record slot is not
+        // read here: the next prefetch may already be filling it)
         const uint32_t* mctl = mplane + (size_t)u * n1 * W;
 #pragma unroll
         for (int q = 0; q < kBCells; ++q) {

@@ -44,13 +44,23 @@ __host__ __device__ inline size_t stencil_u_smem(int nctl) {
 __host__ __device__ inline size_t stencil_prep_smem(int nctl, int nsub) {
     return (size_t)nctl * nsub * 2 * sizeof(float) + (size_t)nctl * (kStencilMaxChk + 1) * 4 + 64;
 }
+// The column table of k_stencil_prep: one word per (control, column).
+__host__ __device__ inline size_t stencil_prep_tab_smem(int nctl, int n2) {
+    return (size_t)nctl * n2 * sizeof(uint32_t);
+}
+constexpr uint32_t kPrepColOff = 0xffffffffu;
 
 // Once per solve.  Block = plane.  Phase A integrates each control once and
 // writes its sweep record; phase B walks (control, row, 32-column word) items
-// and decides admissibility per cell exactly as lookahead does.
+// and decides admissibility per cell exactly as lookahead does.  With
+// `coltab` (columns <= 255), what depends on the column only -- the swept
+// probes' y cells and whether they and the successor's y stay on the table
+// -- is decided once per (control, column) into a shared word of four probe
+// columns (kPrepColOff: off the table), and the per-row walk only adds the x
+// side and the occupancy lookups.  The decisions are the same either way.
 __global__ void __launch_bounds__(256)
     k_stencil_prep(const uint8_t* __restrict__ occ, KParams kp, const float* __restrict__ ctl,
-                   uint32_t* __restrict__ mask, uint32_t* __restrict__ recs) {
+                   uint32_t* __restrict__ mask, uint32_t* __restrict__ recs, int coltab) {
     typedef Ar<float> R_;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nctl = kp.nctl, nsub = kp.nsub, nchk = kp.nchk;
@@ -112,6 +122,75 @@ __global__ void __launch_bounds__(256)
         ap[sc] = R_::div((float)(sc + 1), (float)(nchk > 0 ? nchk : 1));
     const uint8_t* occ_h = occ + (int64_t)i3 * n1 * n2;
     const int64_t items = (int64_t)nctl * n1 * W;
+    if (coltab) {
+        uint32_t* tab = reinterpret_cast<uint32_t*>(smem_raw + stencil_prep_smem(nctl, nsub));
+        for (int32_t it = threadIdx.x; it < nctl * n2; it += blockDim.x) {
+            const int u = it / n2;
+            const int32_t j = it - u * n2;
+            uint32_t word = kPrepColOff;
+            if (sok[u]) {
+                const float y = axisvalue(g, 1, j);
+                float yn = y;
+                for (int k = 0; k < nsub; ++k) yn = R_::add(yn, sy[u * nsub + k]);
+                const float dy = R_::sub(yn, y);
+                bool ok = true;
+                uint32_t packed = 0;
+                for (int sc = 0; sc < nchk && ok; ++sc) {
+                    int32_t cj = 0;
+                    ok = probe_coord(R_::sub(R_::add(y, R_::mul(dy, ap[sc])), lo1), st1, rs1, hy, &cj);
+                    packed |= (uint32_t)cj << (8 * sc);
+                }
+                float f2;
+                if (ok) ok = succ_coord<true>(R_::sub(yn, lo1), st1, rs1, hy, &f2);
+                if (ok) word = packed;
+            }
+            tab[it] = word;
+        }
+        __syncthreads();
+        for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
+            const int u = (int)(it / ((int64_t)n1 * W));
+            const int32_t rem = (int32_t)(it - (int64_t)u * n1 * W);
+            const int32_t i1 = rem / W, w = rem - i1 * W;
+            uint32_t bits = 0;
+            if (sok[u]) {
+                const float x = axisvalue(g, 0, i1);
+                float xn = x;
+                for (int k = 0; k < nsub; ++k) xn = R_::add(xn, sx[u * nsub + k]);
+                const float dx = R_::sub(xn, x);
+                bool xok = true;
+                int32_t ci[kStencilMaxChk];
+                for (int sc = 0; sc < kStencilMaxChk; ++sc) {
+                    ci[sc] = 0;
+                    if (sc < nchk && xok)
+                        xok = probe_coord(R_::sub(R_::add(x, R_::mul(dx, ap[sc])), lo0), st0, rs0,
+                                          hx, &ci[sc]);
+                }
+                float f1;
+                if (xok) xok = succ_coord<true>(R_::sub(xn, lo0), st0, rs0, hx, &f1);
+                if (xok) {
+                    const uint8_t* orow[kStencilMaxChk];
+                    for (int sc = 0; sc < kStencilMaxChk; ++sc)
+                        orow[sc] = sc < nchk
+                                       ? occ + ((int64_t)sck[u * kStencilMaxChk + sc] * n1 + ci[sc]) * n2
+                                       : occ;
+                    const uint32_t* trow = tab + (size_t)u * n2;
+                    for (int b = 0; b < 32; ++b) {
+                        const int32_t j = w * 32 + b;
+                        if (j >= n2) break;
+                        if (occ_h[(int64_t)i1 * n2 + j]) continue;
+                        const uint32_t yw = trow[j];
+                        if (yw == kPrepColOff) continue;
+                        bool ok = true;
+                        for (int sc = 0; sc < nchk && ok; ++sc)
+                            ok = orow[sc][(yw >> (8 * sc)) & 0xffu] == 0;
+                        if (ok) bits |= 1u << b;
+                    }
+                }
+            }
+            mask[((pl * nctl + u) * n1 + i1) * W + w] = bits;
+        }
+        return;
+    }
     for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
         const int u = (int)(it / ((int64_t)n1 * W));
         const int32_t rem = (int32_t)(it - (int64_t)u * n1 * W);
