@@ -213,6 +213,31 @@ int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
 /* Number of this library's kernel launches since the context was created. */
 int pg_launch_count(pg_ctx* ctx, int64_t* launches);
 
+/* ------------------------------------------------------------------ */
+/* adjoint: gradient of a loss on the converged table                  */
+/* ------------------------------------------------------------------ */
+
+typedef struct pg_adjoint_result {
+    int32_t iterations;     /* adjoint sweeps run                              */
+    int32_t active_cells;   /* cells whose backup depends on the model         */
+    double last_residual;   /* L1 change of lambda in the last sweep           */
+    double c_norm;          /* L1 norm of dL/dV                                */
+    double kernel_ms;       /* device time of the adjoint sweeps               */
+} pg_adjoint_result;
+
+/* dL/dtheta for the 18 model entries theta = (B00 B11 B22, A00 A11 A22,
+ * q0 q1 q2, S00 S11 S22, D00 D11 D22, c0 c1 c2) of the loaded problem, at
+ * its current (converged) FP32 table, given dl_dv = dL/dV (ncells floats,
+ * row-major; a device pointer when dl_dv_on_device, else host).  The policy
+ * is the table's argmin (one extra sweep that leaves V unchanged); the
+ * adjoint lambda = dL/dV + P^T lambda is iterated until its L1 change is at
+ * most tol * |dL/dV|_1 or `iters` sweeps ran.  Plain scheme with the masked
+ * stencil's records only (PG_EUNSUPPORTED otherwise).  No counterpart in
+ * the reference, which never differentiates its tables. */
+int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device,
+               int32_t iters, double tol, double* grad18,
+               pg_adjoint_result* res);
+
 /* On-chip ceilings of `device`, measured: shared-memory read bandwidth
  * (GB/s, all SMs), read bandwidth of an L2-resident 64 MiB buffer (GB/s) and
  * FP32 FMA throughput (TFLOP/s).  No counterpart in the reference: the

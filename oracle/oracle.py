@@ -89,6 +89,9 @@ def lib() -> C.CDLL:
     L.og_encode.argtypes = [vp, i64, C.c_int, f64, f32, f64, vp, P(i64), P(i64)]
     L.og_build_occupancy.argtypes = [P(OGrid), C.c_int, vp, vp, f64, C.c_int, vp, C.c_int, f64,
                                      vp, f64, vp]
+    L.og_adjoint_grad_f64.restype = C.c_int
+    L.og_adjoint_grad_f64.argtypes = [vp, vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams), vp, i32,
+                                      f64, C.c_int, vp, P(i32), P(i64)]
     _lib = L
     return L
 
@@ -241,6 +244,25 @@ def build_occupancy(g, polys, margin, robot=None, substeps=3, clearance=0.0, bou
                              0 if robot is None else len(robot), _p(rb), int(substeps),
                              float(clearance), _p(bd), float(wall_clearance), _p(out))
     return out
+
+
+def adjoint_grad_f64(V, pol, occ, g, m, ctl, p, c, iters=20000, tol=1e-10, threads=0):
+    """FP64 reference gradient dL/dtheta (18) of a loss with dL/dV = c on the
+    converged table V (row-major) with policy pol; returns (grad, sweeps,
+    active cells)."""
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    pol = np.ascontiguousarray(pol, dtype=np.int16)
+    occ = np.ascontiguousarray(occ, dtype=np.uint8)
+    ctl = np.ascontiguousarray(ctl, dtype=np.float32)
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    grad = np.zeros(18, dtype=np.float64)
+    it, na = C.c_int32(), C.c_int64()
+    rc = lib().og_adjoint_grad_f64(_p(V), _p(pol), _p(occ), C.byref(g), C.byref(m), _p(ctl),
+                                   int(ctl.size // 3), C.byref(p), _p(c), int(iters), float(tol),
+                                   int(threads), _p(grad), C.byref(it), C.byref(na))
+    if rc != 0:
+        raise MemoryError("og_adjoint_grad_f64 ran out of memory")
+    return grad, it.value, na.value
 
 
 def available_threads() -> int:

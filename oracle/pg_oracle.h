@@ -126,4 +126,13 @@ void og_build_occupancy(const og_grid* g, int npoly, const int* nverts, const do
                         double clearance_cm, const double* bounds, double wall_clearance_cm,
                         uint8_t* out);
 
+/* FP64 reference gradient of a loss on the converged table (pg_oracle_grad.c):
+ * V, pol (-1 = blocked), c = dL/dV row-major; grad gets dL/dtheta for
+ * theta = diagonals of B, A, q, S, D, c (18).  Returns 0, or -1 if out of
+ * memory. */
+int og_adjoint_grad_f64(const double* V, const int16_t* pol, const uint8_t* occ, const og_grid* g,
+                        const og_model* m, const float* ctl, int32_t nctl, const og_params* p,
+                        const double* c, int32_t iters, double tol, int threads, double* grad,
+                        int32_t* iters_done, int64_t* nactive);
+
 #endif

@@ -1,0 +1,471 @@
+// pg_adjoint.cuh -- gradient of a loss on the converged value table with
+// respect to the drivetrain model (included inside namespace pg by
+// pg_kernels.cu, after pg_stencil_u.cuh).
+//
+// At the converged table V and its policy pi (the argmin control of each
+// cell), the plain scheme's fixed point reads, for every active cell
+// (free, not a target, not clipped to the cap),
+//     V(s) = tau + I(V, x*(s, pi(s); theta)),
+// I the 64-corner multilinear interpolant (PeregrineSolver.jl:399-466) and
+// x* the successor of lookahead (PeregrineSolver.jl:1100-1153).  With the
+// policy held fixed (the derivative of a min is the derivative at its
+// argmin), dV/dtheta = P dV/dtheta + g_theta, P the interpolation weights of
+// the successors and g_theta(s) = grad_x I(V, x*) . dx*/dtheta.  For a loss
+// L(V) with c = dL/dV the adjoint lambda = c + P^T lambda gives
+//     dL/dtheta = lambda^T g_theta.
+// No counterpart in the reference: it never differentiates its tables.
+//
+// theta is the 18 model entries a drivetrain fit moves most: the diagonals
+// of B, A, S, D and the vectors q and c, in that order (B00 B11 B22, A00
+// A11 A22, q0 q1 q2, S00 S11 S22, D00 D11 D22, c0 c1 c2).  The successor's
+// derivative comes from forward-mode dual numbers through the same RK2 /
+// Euler substeps; by position invariance it depends on (plane, control)
+// only, so each block computes it once per control.
+
+constexpr int kNTheta = 18;
+
+// A value with its derivatives along the 18 model entries.
+struct Dual {
+    double v;
+    double d[kNTheta];
+};
+
+__device__ __forceinline__ Dual dconst(double v) {
+    Dual r;
+    r.v = v;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) r.d[k] = 0.0;
+    return r;
+}
+__device__ __forceinline__ Dual dadd(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v + b.v;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) r.d[k] = a.d[k] + b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dual dsub(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v - b.v;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) r.d[k] = a.d[k] - b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dual dmul(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v * b.v;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return r;
+}
+__device__ __forceinline__ Dual dscale(const Dual& a, double s) {
+    Dual r;
+    r.v = a.v * s;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) r.d[k] = a.d[k] * s;
+    return r;
+}
+// a + b * s (s a constant)
+__device__ __forceinline__ Dual daxpy(const Dual& a, const Dual& b, double s) {
+    Dual r;
+    r.v = a.v + b.v * s;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) r.d[k] = a.d[k] + b.d[k] * s;
+    return r;
+}
+__device__ __forceinline__ void dsincos(const Dual& a, Dual* s, Dual* c) {
+    double sv, cv;
+    sincos(a.v, &sv, &cv);
+    s->v = sv;
+    c->v = cv;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) {
+        s->d[k] = cv * a.d[k];
+        c->d[k] = -sv * a.d[k];
+    }
+}
+// csign (PeregrineSolver.jl:113): clamp(v / eps, -1, 1)
+__device__ __forceinline__ Dual dcsign(const Dual& a, double e) {
+    const double q = a.v / e;
+    if (q >= 1.0) return dconst(1.0);
+    if (q <= -1.0) return dconst(-1.0);
+    return dscale(a, 1.0 / e);
+}
+// |v| v
+__device__ __forceinline__ Dual dabsmul(const Dual& a) {
+    Dual r;
+    r.v = fabs(a.v) * a.v;
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) r.d[k] = 2.0 * fabs(a.v) * a.d[k];
+    return r;
+}
+
+// theta index of model entry (block, row, col), or -1 when it is held fixed.
+__device__ __forceinline__ int theta_index(int blk, int r, int c) {
+    // blk: 0 B, 1 A, 2 q, 3 S, 4 D, 5 c (q and c: c == 0)
+    if (blk == 2 || blk == 5) return 3 * blk + r;
+    if (r != c) return -1;
+    return 3 * blk + r;
+}
+
+__device__ __forceinline__ Dual dparam(double v, int idx) {
+    Dual r = dconst(v);
+    if (idx >= 0) r.d[idx] = 1.0;
+    return r;
+}
+
+// body_accel_sat (PeregrineSolver.jl:151-163) with dual state and model.
+__device__ void daccel(const pg_model& m, double u1, double u2, double u3, const Dual& vx,
+                       const Dual& vy, const Dual& w, Dual* a) {
+    const Dual w2 = dmul(w, w);
+    const Dual sg[3] = {dcsign(vx, m.eps[0]), dcsign(vy, m.eps[1]), dcsign(w, m.eps[2])};
+    const Dual dd[3] = {dabsmul(vx), dabsmul(vy), dabsmul(w)};
+    const Dual* v[3] = {&vx, &vy, &w};
+    const double u[3] = {u1, u2, u3};
+    for (int r = 0; r < 3; ++r) {
+        Dual s = dconst(0.0);
+        for (int c = 0; c < 3; ++c) {
+            s = dadd(s, dscale(dparam(m.B[3 * r + c], theta_index(0, r, c)), u[c]));
+        }
+        for (int c = 0; c < 3; ++c) s = dadd(s, dmul(dparam(m.A[3 * r + c], theta_index(1, r, c)), *v[c]));
+        s = dadd(s, dmul(dparam(m.q[r], theta_index(2, r, 0)), w2));
+        for (int c = 0; c < 3; ++c) s = dadd(s, dmul(dparam(m.S[3 * r + c], theta_index(3, r, c)), sg[c]));
+        for (int c = 0; c < 3; ++c) s = dadd(s, dmul(dparam(m.D[3 * r + c], theta_index(4, r, c)), dd[c]));
+        s = dadd(s, dparam(m.c[r], theta_index(5, r, 0)));
+        a[r] = s;
+    }
+}
+
+// The successor of one (plane, control) in interpolation coordinates, with
+// its derivatives: position offset (x, y), heading, field-frame velocity,
+// turn rate.  Mirrors integrate() (PeregrineSolver.jl:203-279) in double.
+__device__ void dual_successor(const pg_model& m, const pg_params& p, double h0, double vfx,
+                               double vfy, double w0, double u1r, double u2r, double u3r,
+                               double tau, int nsub, Dual* out6) {
+    // traction saturation depends on the command only
+    double gn = 1.0;
+    if (!(isnan(m.knee) || m.knee <= 0.0f)) {
+        const double mg = sqrt(u1r * u1r + u2r * u2r + u3r * u3r);
+        const double r = mg / (double)m.knee;
+        if (r >= 1.0e-6) gn = tanh(r) / r;
+    }
+    const double u1 = u1r * gn, u2 = u2r * gn, u3 = u3r * gn;
+    double s0, c0;
+    sincos(h0, &s0, &c0);
+    Dual x = dconst(0.0), y = dconst(0.0), h = dconst(h0);
+    Dual vx = dconst(c0 * vfx + s0 * vfy), vy = dconst(-s0 * vfx + c0 * vfy), w = dconst(w0);
+    const double hs = tau / nsub, hh = 0.5 * hs;
+    for (int k = 0; k < nsub; ++k) {
+        Dual a[3], sh, ch;
+        daccel(m, u1, u2, u3, vx, vy, w, a);
+        dsincos(h, &sh, &ch);
+        const Dual d1x = dsub(dmul(ch, vx), dmul(sh, vy));
+        const Dual d1y = dadd(dmul(sh, vx), dmul(ch, vy));
+        const Dual d1vx = dadd(a[0], dmul(w, vy));
+        const Dual d1vy = dsub(a[1], dmul(w, vx));
+        if (!p.rk2) {
+            x = daxpy(x, d1x, hs);
+            y = daxpy(y, d1y, hs);
+            h = daxpy(h, w, hs);
+            vx = daxpy(vx, d1vx, hs);
+            vy = daxpy(vy, d1vy, hs);
+            w = daxpy(w, a[2], hs);
+        } else {
+            const Dual mh = daxpy(h, w, hh);
+            const Dual mvx = daxpy(vx, d1vx, hh), mvy = daxpy(vy, d1vy, hh);
+            const Dual mw = daxpy(w, a[2], hh);
+            daccel(m, u1, u2, u3, mvx, mvy, mw, a);
+            dsincos(mh, &sh, &ch);
+            const Dual d2x = dsub(dmul(ch, mvx), dmul(sh, mvy));
+            const Dual d2y = dadd(dmul(sh, mvx), dmul(ch, mvy));
+            const Dual d2vx = dadd(a[0], dmul(mw, mvy));
+            const Dual d2vy = dsub(a[1], dmul(mw, mvx));
+            x = daxpy(x, d2x, hs);
+            y = daxpy(y, d2y, hs);
+            h = daxpy(h, mw, hs);
+            vx = daxpy(vx, d2vx, hs);
+            vy = daxpy(vy, d2vy, hs);
+            w = daxpy(w, a[2], hs);
+        }
+    }
+    Dual sh, ch;
+    dsincos(h, &sh, &ch);
+    out6[0] = x;
+    out6[1] = y;
+    out6[2] = h;
+    out6[3] = dsub(dmul(ch, vx), dmul(sh, vy));
+    out6[4] = dadd(dmul(sh, vx), dmul(ch, vy));
+    out6[5] = w;
+}
+
+// The successor's lower corner and fraction along x (ax 0) or y (ax 1) of
+// a cell in row/column idx, rounded as the reference rounds it; false when
+// the successor is off the table.
+__device__ __forceinline__ bool succ_axis(const GridT<float>& g, int ax, int32_t idx,
+                                          const float* inc, int nsub, int32_t* lo, float* t) {
+    typedef Ar<float> R_;
+    const float x = ax == 0 ? axisvalue(g, 0, idx) : axisvalue(g, 1, idx);
+    const float l = ax == 0 ? g.lo[0] : g.lo[1];
+    const float st = ax == 0 ? g.step[0] : g.step[1];
+    const int32_t n = ax == 0 ? g.n[0] : g.n[1];
+    float xn = x;
+    for (int k = 0; k < nsub; ++k) xn = R_::add(xn, inc[k]);
+    const float f = R_::div(R_::sub(xn, l), st);
+    if (!(f >= 0.0f && f <= (float)(n - 1))) return false;
+    const float fl = floorf(f);
+    *lo = (int32_t)fl;
+    *t = R_::sub(f, fl);
+    return true;
+}
+
+// The plane-major indices and weights of the 64 interpolation corners of a
+// cell's successor under control record `rec`; false when the cell's
+// successor is off the table.
+__device__ __forceinline__ bool succ_corners(const GridT<float>& g, int64_t P, const uint32_t* rec,
+                                             int32_t i, int32_t j, int32_t* rr, int32_t* cc,
+                                             float* tx, float* ty) {
+    const int nsub = (int)rec[kUNT + 19];
+    const float* incx = reinterpret_cast<const float*>(rec + kUInc);
+    if (!succ_axis(g, 0, i, incx, nsub, rr, tx)) return false;
+    if (!succ_axis(g, 1, j, incx + kStencilMaxSub, nsub, cc, ty)) return false;
+    return true;
+}
+
+// Active cells: free, 0 < V < cap, policy admissible (mask bit) and the
+// policy's backup not clipped to the cap.  V plane-major FP32.
+__global__ void k_adj_active(const float* __restrict__ V, const int16_t* __restrict__ pol,
+                             const uint8_t* __restrict__ occ, const uint32_t* __restrict__ mask,
+                             const uint32_t* __restrict__ recs, KParams kp,
+                             uint8_t* __restrict__ active) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= kp.ncells) return;
+    const Layout L = make_layout(kp);
+    GridT<float> g;
+    load_grid(g, kp.g);
+    const int64_t pl = e / L.P;
+    const int32_t r = (int32_t)(e - pl * L.P);
+    const int32_t i = r / L.n[1], j = r - i * L.n[1];
+    int64_t pp = pl;
+    const int32_t i6 = (int32_t)(pp % L.n[5]); pp /= L.n[5];
+    const int32_t i5 = (int32_t)(pp % L.n[4]); pp /= L.n[4];
+    const int32_t i4 = (int32_t)(pp % L.n[3]); pp /= L.n[3];
+    const int32_t i3 = (int32_t)pp;
+    uint8_t act = 0;
+    const float cap = kp.p.cap;
+    const float v = V[e];
+    const int u = pol[L.rowmajor(i, j, i3, i4, i5, i6)];
+    if (u >= 0 && occ[L.occ(i, j, i3)] == 0 && v > 0.0f && v < cap) {
+        const int32_t W = mask_words(L.n[1]);
+        const uint32_t mw = mask[((pl * kp.nctl + u) * L.n[0] + i) * W + (j >> 5)];
+        if ((mw >> (j & 31)) & 1u) {
+            const uint32_t* rec = recs + ((size_t)pl * kp.nctl + u) * kURec;
+            int32_t r0, c0;
+            float tx, ty;
+            if (succ_corners(g, L.P, rec, i, j, &r0, &c0, &tx, &ty)) {
+                const int32_t r1 = min(r0 + 1, L.n[0] - 1), c1 = min(c0 + 1, L.n[1] - 1);
+                float acc = 0.0f;
+                for (int c = 0; c < 16; ++c) {
+                    const float w = __uint_as_float(rec[c]);
+                    const float* Vc = V + (int64_t)rec[kUNT + c] * L.P;
+                    const float a = (1.0f - tx) * Vc[r0 * L.n[1] + c0] + tx * Vc[r1 * L.n[1] + c0];
+                    const float b = (1.0f - tx) * Vc[r0 * L.n[1] + c1] + tx * Vc[r1 * L.n[1] + c1];
+                    acc += w * ((1.0f - ty) * a + ty * b);
+                }
+                const float tau = __uint_as_float(rec[16]);
+                if (acc < cap && tau + acc < cap) act = 1;
+            }
+        }
+    }
+    active[e] = act;
+}
+
+// lambda_out += P^T lambda_in over the active cells (lambda_out holds c on
+// entry).  One thread per cell; 64 atomic adds per active cell with a
+// nonzero lambda.
+__global__ void k_adj_scatter(const float* __restrict__ lam_in, float* __restrict__ lam_out,
+                              const int16_t* __restrict__ pol, const uint8_t* __restrict__ active,
+                              const uint32_t* __restrict__ recs, KParams kp) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= kp.ncells) return;
+    const float lv = lam_in[e];
+    if (lv == 0.0f || !active[e]) return;
+    const Layout L = make_layout(kp);
+    GridT<float> g;
+    load_grid(g, kp.g);
+    const int64_t pl = e / L.P;
+    const int32_t r = (int32_t)(e - pl * L.P);
+    const int32_t i = r / L.n[1], j = r - i * L.n[1];
+    int64_t pp = pl;
+    const int32_t i6 = (int32_t)(pp % L.n[5]); pp /= L.n[5];
+    const int32_t i5 = (int32_t)(pp % L.n[4]); pp /= L.n[4];
+    const int32_t i4 = (int32_t)(pp % L.n[3]); pp /= L.n[3];
+    const int32_t i3 = (int32_t)pp;
+    const int u = pol[L.rowmajor(i, j, i3, i4, i5, i6)];
+    const uint32_t* rec = recs + ((size_t)pl * kp.nctl + u) * kURec;
+    int32_t r0, c0;
+    float tx, ty;
+    if (!succ_corners(g, L.P, rec, i, j, &r0, &c0, &tx, &ty)) return;
+    const int32_t r1 = min(r0 + 1, L.n[0] - 1), c1 = min(c0 + 1, L.n[1] - 1);
+    const float wxy[4] = {(1.0f - tx) * (1.0f - ty), tx * (1.0f - ty), (1.0f - tx) * ty, tx * ty};
+    const int32_t off[4] = {r0 * L.n[1] + c0, r1 * L.n[1] + c0, r0 * L.n[1] + c1, r1 * L.n[1] + c1};
+    for (int c = 0; c < 16; ++c) {
+        const float w = __uint_as_float(rec[c]) * lv;
+        if (w == 0.0f) continue;
+        float* dst = lam_out + (int64_t)rec[kUNT + c] * L.P;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (wxy[q] != 0.0f) atomicAdd(dst + off[q], w * wxy[q]);
+    }
+}
+
+// sum |a - b| into per-block partials (the adjoint's convergence signal)
+__global__ void k_adj_diff(const float* __restrict__ a, const float* __restrict__ b, int64_t n,
+                           double* part_sum, double* part_max) {
+    double s = 0.0, m = 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const double d = fabs((double)a[k] - (double)b[k]);
+        s += d;
+        m = fmax(m, d);
+    }
+    block_partial(s, m, part_sum, part_max);
+}
+
+// number of active cells into per-block partials
+__global__ void k_adj_count(const uint8_t* __restrict__ a, int64_t n, double* part_sum,
+                            double* part_max) {
+    double s = 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x)
+        s += a[k] ? 1.0 : 0.0;
+    block_partial(s, 0.0, part_sum, part_max);
+}
+
+// shared memory of k_adj_grad: per control, its transition corners and
+// fractions and the successor's derivatives
+__host__ __device__ inline size_t adj_grad_smem(int nctl) {
+    return (size_t)nctl * (8 * sizeof(int32_t) + 6 * kNTheta * sizeof(float) + 4 * sizeof(float));
+}
+
+// dL/dtheta = sum over active cells of lambda(s) grad_x I(V, x*) . dx*/dtheta.
+// Block = plane: phase A computes, per control, the transition (corners and
+// fractions, exactly as the forward sweep) and the dual successor; phase B
+// walks the plane's cells.  The 18 sums go to `grad` with double atomics.
+__global__ void __launch_bounds__(128)
+    k_adj_grad(const float* __restrict__ V, const float* __restrict__ lam,
+               const int16_t* __restrict__ pol, const uint8_t* __restrict__ active,
+               const uint32_t* __restrict__ recs, KParams kp, const float* __restrict__ ctl,
+               double* __restrict__ grad) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nctl = kp.nctl;
+    int32_t* sjb = reinterpret_cast<int32_t*>(smem_raw);           // [nctl][4]
+    int32_t* sok = sjb + 4 * nctl;                                  // [nctl][4] (ok, pad)
+    float* stt = reinterpret_cast<float*>(sok + 4 * nctl);          // [nctl][4]
+    float* sD = stt + 4 * nctl;                                     // [nctl][6][18]
+    const Layout L = make_layout(kp);
+    GridT<float> g;
+    load_grid(g, kp.g);
+    const int64_t pl = blockIdx.x;
+    int64_t pp = pl;
+    const int32_t i6 = (int32_t)(pp % L.n[5]); pp /= L.n[5];
+    const int32_t i5 = (int32_t)(pp % L.n[4]); pp /= L.n[4];
+    const int32_t i4 = (int32_t)(pp % L.n[3]); pp /= L.n[3];
+    const int32_t i3 = (int32_t)pp;
+    const int64_t P = L.P;
+
+    // any work in this plane?
+    int any = 0;
+    for (int64_t k = threadIdx.x; k < P; k += blockDim.x)
+        any |= (active[pl * P + k] && lam[pl * P + k] != 0.0f);
+    if (!__syncthreads_or(any)) return;
+
+    for (int u = threadIdx.x; u < nctl; u += blockDim.x) {
+        Transition<float> t;
+        transition(kp, g, i3, i4, i5, i6, ctl, u, t);
+        for (int k = 0; k < 4; ++k) {
+            sjb[4 * u + k] = t.jb[k];
+            stt[4 * u + k] = t.tt[k];
+            sok[4 * u + k] = 0;
+        }
+        sok[4 * u] = t.ok ? 1 : 0;
+        Dual s6[6];
+        if (t.ok) {
+            dual_successor(kp.m, kp.p, (double)axisvalue(g, 2, i3), (double)axisvalue(g, 3, i4),
+                           (double)axisvalue(g, 4, i5), (double)axisvalue(g, 5, i6),
+                           (double)ctl[u], (double)ctl[u + nctl], (double)ctl[u + 2 * nctl],
+                           (double)t.tau, kp.nsub, s6);
+        } else {
+            for (int a = 0; a < 6; ++a) s6[a] = dconst(0.0);
+        }
+        for (int a = 0; a < 6; ++a)
+            for (int k = 0; k < kNTheta; ++k) sD[((size_t)u * 6 + a) * kNTheta + k] = (float)s6[a].d[k];
+    }
+    __syncthreads();
+
+    float acc[kNTheta];
+#pragma unroll
+    for (int k = 0; k < kNTheta; ++k) acc[k] = 0.0f;
+    const float inv_step[6] = {1.0f / g.step[0], 1.0f / g.step[1], 1.0f / g.step[2],
+                               1.0f / g.step[3], 1.0f / g.step[4], 1.0f / g.step[5]};
+    for (int64_t k = threadIdx.x; k < P; k += blockDim.x) {
+        const int64_t e = pl * P + k;
+        if (!active[e]) continue;
+        const float lv = lam[e];
+        if (lv == 0.0f) continue;
+        const int32_t i = (int32_t)(k / L.n[1]), j = (int32_t)(k - (int64_t)i * L.n[1]);
+        const int u = pol[L.rowmajor(i, j, i3, i4, i5, i6)];
+        if (!sok[4 * u]) continue;
+        const uint32_t* rec = recs + ((size_t)pl * nctl + u) * kURec;
+        int32_t r0, c0;
+        float tx, ty;
+        if (!succ_corners(g, P, rec, i, j, &r0, &c0, &tx, &ty)) continue;
+        int32_t ib[6] = {r0, c0, sjb[4 * u], sjb[4 * u + 1], sjb[4 * u + 2], sjb[4 * u + 3]};
+        float tt[6] = {tx, ty, stt[4 * u], stt[4 * u + 1], stt[4 * u + 2], stt[4 * u + 3]};
+        // gradient of the multilinear interpolant along its 6 fractions
+        float gI[6] = {0, 0, 0, 0, 0, 0};
+        for (int d = 0; d < 64; ++d) {
+            int32_t jj[6];
+            float a[6];
+#pragma unroll
+            for (int ax = 0; ax < 6; ++ax) {
+                const int bit = (d >> ax) & 1;
+                a[ax] = bit ? tt[ax] : 1.0f - tt[ax];
+                if (ax == 2)
+                    jj[ax] = (ib[ax] + bit) % L.n[2];
+                else
+                    jj[ax] = min(ib[ax] + bit, L.n[ax] - 1);
+            }
+            const float vd = V[L.dev(jj[0], jj[1], jj[2], jj[3], jj[4], jj[5])];
+#pragma unroll
+            for (int ax = 0; ax < 6; ++ax) {
+                float pr = ((d >> ax) & 1) ? vd : -vd;
+#pragma unroll
+                for (int o = 0; o < 6; ++o)
+                    if (o != ax) pr *= a[o];
+                gI[ax] += pr;
+            }
+        }
+        const float* D = sD + (size_t)u * 6 * kNTheta;
+#pragma unroll
+        for (int ax = 0; ax < 6; ++ax) {
+            const float ga = lv * gI[ax] * inv_step[ax];
+#pragma unroll
+            for (int q = 0; q < kNTheta; ++q) acc[q] = fmaf(ga, D[ax * kNTheta + q], acc[q]);
+        }
+    }
+    // block sum of the 18 partial gradients, then one double atomic each
+    __shared__ float red[kNTheta][4];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kNTheta; ++q) {
+        float v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0 && wid < 4) red[q][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kNTheta) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32 && w < 4; ++w) s += red[threadIdx.x][w];
+        atomicAdd(grad + threadIdx.x, s);
+    }
+}

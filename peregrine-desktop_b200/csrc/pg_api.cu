@@ -771,6 +771,137 @@ int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
     return PG_OK;
 }
 
+int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t iters,
+               double tol, double* grad18, pg_adjoint_result* res) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (!dl_dv || !grad18) return fail(PG_EINVAL, "null argument");
+    if (!ctx->stencil_ok || !ctx->mask_ok)
+        return fail(PG_EUNSUPPORTED, "the adjoint needs the plain scheme with the masked stencil's "
+                                     "records (" + (ctx->stencil_ok ? std::string("not enough device "
+                                     "memory for them") : ctx->stencil_why) + ")");
+    if (ctx->storage != PG_STORE_F32)
+        return fail(PG_EUNSUPPORTED, "the adjoint runs on an FP32 table");
+    const pg::KParams& kp = ctx->kp;
+    const int64_t n = kp.ncells;
+    if (!ctx->argmin_d)
+        PG_CUDA(cudaMalloc(&ctx->argmin_d, (size_t)n * sizeof(int16_t)));
+    float* lam[2] = {nullptr, nullptr};
+    float* c = nullptr;
+    uint8_t* active = nullptr;
+    double* grad_d = nullptr;
+    auto release = [&]() {
+        if (lam[0]) cudaFree(lam[0]);
+        if (lam[1]) cudaFree(lam[1]);
+        if (c) cudaFree(c);
+        if (active) cudaFree(active);
+        if (grad_d) cudaFree(grad_d);
+    };
+    auto cuda_fail = [&](cudaError_t e, const char* what) {
+        release();
+        return fail(e == cudaErrorMemoryAllocation ? PG_ENOMEM : PG_ECUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaMalloc(&lam[0], (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&lam[1], (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&c, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&active, (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&grad_d, pg::kNThetaHost * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint buffers");
+
+    // the policy: one sweep with argmin into the spare buffer, V untouched
+    pg::SweepBufs sb{ctx->part_sum, ctx->part_max, ctx->nparts, ctx->red_d};
+    const void* vin = ctx->V[ctx->cur];
+    void* spare = ctx->V[1 - ctx->cur];
+    if (ctx->blend_ok)
+        e = pg::launch_stencil_b(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
+                                 kp, ctx->order_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
+    else if (ctx->gather_ok)
+        e = pg::launch_stencil_u(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
+                                 kp, ctx->order_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
+    else
+        e = pg::launch_stencil(ctx->storage, false, vin, spare, ctx->occ_d, kp, ctx->ctl_d,
+                               ctx->order_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
+    if (e != cudaSuccess) return cuda_fail(e, "policy sweep");
+
+    double dm0 = 0.0;
+    // c = dL/dV in the device layout
+    if (dl_dv_on_device) {
+        e = pg::launch_from_rowmajor(PG_STORE_F32, dl_dv, c, kp, ctx->stream);
+    } else {
+        rc = ensure_stage(ctx);
+        if (rc) { release(); return rc; }
+        e = cudaMemcpyAsync(ctx->stage_d, dl_dv, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = pg::launch_from_rowmajor(PG_STORE_F32, ctx->stage_d, c, kp, ctx->stream);
+    }
+    ctx->launches += 1;
+    if (e == cudaSuccess)
+        e = pg::launch_adj_active((const float*)vin, ctx->argmin_d, ctx->occ_d, ctx->mask_d,
+                                  ctx->recs_d, kp, active, ctx->stream);
+    ctx->launches += 1;
+    double nact = 0.0;
+    if (e == cudaSuccess) e = pg::launch_adj_count(active, n, sb, ctx->stream);
+    ctx->launches += 2;
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint set-up");
+    rc = read_residual(ctx, &nact, &dm0);
+    if (rc) { release(); return rc; }
+    if (e == cudaSuccess) e = cudaMemsetAsync(lam[1], 0, (size_t)n * 4, ctx->stream);
+    if (e == cudaSuccess) e = pg::launch_adj_diff(c, lam[1], n, sb, ctx->stream);
+    ctx->launches += 2;
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint set-up");
+    double cn = 0.0, dm = 0.0;
+    rc = read_residual(ctx, &cn, &dm);
+    if (rc) { release(); return rc; }
+
+    // lambda <- c + P^T lambda until quiet
+    e = cudaMemcpyAsync(lam[0], c, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint set-up");
+    int cur = 0, done = 0;
+    double r = INFINITY, kms = 0.0;
+    for (int32_t it = 1; it <= iters && cn > 0.0; ++it) {
+        float* lin = lam[cur];
+        float* lout = lam[1 - cur];
+        PG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+        e = cudaMemcpyAsync(lout, c, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = pg::launch_adj_scatter(lin, lout, ctx->argmin_d, active, ctx->recs_d, kp, ctx->stream);
+        if (e == cudaSuccess) e = pg::launch_adj_diff(lout, lin, n, sb, ctx->stream);
+        ctx->launches += 3;
+        if (e != cudaSuccess) return cuda_fail(e, "adjoint sweep");
+        PG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+        rc = read_residual(ctx, &r, &dm);
+        if (rc) { release(); return rc; }
+        float ms = 0.0f;
+        PG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        kms += ms;
+        cur = 1 - cur;
+        done = it;
+        if (r <= tol * cn) break;
+    }
+
+    // dL/dtheta = lambda^T g_theta
+    e = cudaMemsetAsync(grad_d, 0, pg::kNThetaHost * sizeof(double), ctx->stream);
+    if (e == cudaSuccess)
+        e = pg::launch_adj_grad((const float*)vin, lam[cur], ctx->argmin_d, active, ctx->recs_d, kp,
+                                ctx->ctl_d, grad_d, ctx->stream);
+    ctx->launches += 1;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(grad18, grad_d, pg::kNThetaHost * sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint gradient");
+    if (res) {
+        std::memset(res, 0, sizeof(*res));
+        res->iterations = done;
+        res->last_residual = r;
+        res->c_norm = cn;
+        res->kernel_ms = kms;
+        res->active_cells = (int32_t)nact;
+    }
+    release();
+    return PG_OK;
+}
+
 int pg_launch_count(pg_ctx* ctx, int64_t* launches) {
     if (!ctx || !launches) return fail(PG_EINVAL, "null argument");
     *launches = ctx->launches;

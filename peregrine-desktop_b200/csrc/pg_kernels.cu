@@ -554,6 +554,7 @@ __global__ void __launch_bounds__(kCellThreads)
 #include "pg_stencil.cuh"
 #include "pg_stencil_u.cuh"
 #include "pg_stencil_b.cuh"
+#include "pg_adjoint.cuh"
 
 // ---------------------------------------------------------------------------
 // Encoding (encode_into!, Pipeline.jl:698-780), from the device layout into
@@ -923,6 +924,51 @@ size_t stencil_b_smem_bytes(const KParams& kp) {
     return stencil_b_smem(kp.nctl, kp.btile_x, kp.g.n[1]);
 }
 size_t stencil_u_smem_bytes(const KParams& kp) { return stencil_u_smem(kp.nctl); }
+
+cudaError_t launch_adj_active(const float* V, const int16_t* pol, const uint8_t* occ,
+                              const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                              uint8_t* active, cudaStream_t st) {
+    k_adj_active<<<grid_for(kp.ncells, 256), 256, 0, st>>>(V, pol, occ, mask, recs, kp, active);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_scatter(const float* lam_in, float* lam_out, const int16_t* pol,
+                               const uint8_t* active, const uint32_t* recs, const KParams& kp,
+                               cudaStream_t st) {
+    k_adj_scatter<<<grid_for(kp.ncells, 256), 256, 0, st>>>(lam_in, lam_out, pol, active, recs, kp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_diff(const float* a, const float* b, int64_t n, const SweepBufs& sb,
+                            cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(sb.nparts, 148 * 16);
+    k_adj_diff<<<(unsigned)blocks, 256, 0, st>>>(a, b, n, sb.part_sum, sb.part_max);
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_count(const uint8_t* a, int64_t n, const SweepBufs& sb, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(sb.nparts, 148 * 16);
+    k_adj_count<<<(unsigned)blocks, 256, 0, st>>>(a, n, sb.part_sum, sb.part_max);
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_grad(const float* V, const float* lam, const int16_t* pol,
+                            const uint8_t* active, const uint32_t* recs, const KParams& kp,
+                            const float* ctl, double* grad, cudaStream_t st) {
+    const size_t smem = adj_grad_smem(kp.nctl);
+    if (smem > 200 * 1024 || kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_adj_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_adj_grad<<<(unsigned)kp.nplanes, 128, smem, st>>>(V, lam, pol, active, recs, kp, ctl, grad);
+    return cudaGetLastError();
+}
 
 size_t stencil_recs_bytes(const KParams& kp) {
     return (size_t)kp.nplanes * kp.nctl * kURec * sizeof(uint32_t);

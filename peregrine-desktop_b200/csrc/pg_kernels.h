@@ -45,6 +45,18 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
                              const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                              cudaStream_t st, int64_t* launches);
 size_t stencil_b_smem_bytes(const KParams& kp);
+cudaError_t launch_adj_active(const float* V, const int16_t* pol, const uint8_t* occ,
+                              const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                              uint8_t* active, cudaStream_t st);
+cudaError_t launch_adj_scatter(const float* lam_in, float* lam_out, const int16_t* pol,
+                               const uint8_t* active, const uint32_t* recs, const KParams& kp,
+                               cudaStream_t st);
+cudaError_t launch_adj_diff(const float* a, const float* b, int64_t n, const SweepBufs& sb,
+                            cudaStream_t st);
+cudaError_t launch_adj_count(const uint8_t* a, int64_t n, const SweepBufs& sb, cudaStream_t st);
+cudaError_t launch_adj_grad(const float* V, const float* lam, const int16_t* pol,
+                            const uint8_t* active, const uint32_t* recs, const KParams& kp,
+                            const float* ctl, double* grad, cudaStream_t st);
 size_t stencil_u_smem_bytes(const KParams& kp);
 size_t stencil_recs_bytes(const KParams& kp);
 size_t stencil_mask_bytes(const KParams& kp);

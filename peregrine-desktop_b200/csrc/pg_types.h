@@ -17,6 +17,8 @@ constexpr int kCellThreads = 128;
 // Blend-then-shift sweep: cells per thread, cells per block at most.
 constexpr int kBCells = 4;
 constexpr int kBMaxTileCells = 1024;
+// Model entries the adjoint differentiates (diagonals of B, A, S, D; q; c).
+constexpr int kNThetaHost = 18;
 
 // Everything a sweep kernel needs besides the arrays, passed by value.
 struct KParams {

@@ -31,7 +31,7 @@ EXPORTS = (
     "pg_abi_version", "pg_last_error", "pg_default_opts", "pg_create", "pg_destroy",
     "pg_solve_value", "pg_load_problem", "pg_solve", "pg_get_value", "pg_set_value",
     "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
-    "pg_launch_count", "pg_measure_peaks", "pg_sweep_noalloc",
+    "pg_launch_count", "pg_adjoint", "pg_measure_peaks", "pg_sweep_noalloc",
 )
 
 
@@ -75,6 +75,12 @@ class SolveResult(C.Structure):
                 ("cell_controls", C.c_int64)]
 
 
+class AdjointResult(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("active_cells", C.c_int32),
+                ("last_residual", C.c_double), ("c_norm", C.c_double),
+                ("kernel_ms", C.c_double)]
+
+
 PROGRESS_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_double, C.c_double)
 
 _lib = None
@@ -113,6 +119,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "pg_encode": (C.c_int, [vp, i32, f64, f64, i64, i64, vp, P(i64), P(i64)]),
         "pg_time_sweeps": (C.c_int, [vp, i32, i32, i32, P(f64)]),
         "pg_launch_count": (C.c_int, [vp, P(i64)]),
+        "pg_adjoint": (C.c_int, [vp, vp, i32, i32, f64, vp, P(AdjointResult)]),
         "pg_measure_peaks": (C.c_int, [C.c_int, P(f64), P(f64), P(f64)]),
         "pg_sweep_noalloc": (C.c_int, [P(Grid6), P(Model), P(Params), vp, vp, i32, vp, vp, i32,
                                        vp, P(f64), P(f64)]),
@@ -249,6 +256,22 @@ class Context:
         _check(self._lib.pg_time_sweeps(self._h, int(warmup), int(steps), int(kernel),
                                         C.byref(ms)))
         return ms.value
+
+    def adjoint(self, dl_dv, iters: int = 20000, tol: float = 1e-5):
+        """dL/dtheta (18 model entries) at the current converged FP32 table for
+        dl_dv = dL/dV (row-major: a host array, or a device address as int)."""
+        grad = np.zeros(18, dtype=np.float64)
+        res = AdjointResult()
+        if isinstance(dl_dv, int):
+            ptr, on_dev = C.c_void_p(dl_dv), 1
+        else:
+            dl_dv = np.ascontiguousarray(dl_dv, dtype=np.float32)
+            if dl_dv.size != self.ncells:
+                raise ValueError("dL/dV has the wrong size")
+            ptr, on_dev = _ptr(dl_dv), 0
+        _check(self._lib.pg_adjoint(self._h, ptr, on_dev, int(iters), float(tol), _ptr(grad),
+                                    C.byref(res)))
+        return grad, res
 
     def launch_count(self) -> int:
         n = C.c_int64()

@@ -146,3 +146,9 @@ def test_library_refuses_bad_arguments_without_a_gpu():
     assert lib.pg_destroy(None) == 0
     assert lib.pg_create(None, 0) == _lib.PG_EINVAL
     assert b"null" in lib.pg_last_error()
+    # the adjoint binding converts its arguments and refuses a null context
+    grad = np.zeros(18)
+    res = _lib.AdjointResult()
+    dl = np.zeros(4, dtype=np.float32)
+    assert lib.pg_adjoint(None, dl.ctypes.data, 0, 10, 1e-6, grad.ctypes.data,
+                          C.byref(res)) == _lib.PG_EINVAL
