@@ -213,6 +213,53 @@ int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
 /* Number of this library's kernel launches since the context was created. */
 int pg_launch_count(pg_ctx* ctx, int64_t* launches);
 
+/* Rows of one plane per block of the blend-then-shift sweep (the tile
+ * shape the autotuner picks): 1 <= rows <= Nx and rows * Ny <= 1024.  No
+ * counterpart in the reference (its kernel has one thread per cell). */
+int pg_set_tile_rows(pg_ctx* ctx, int32_t rows);
+
+/* ------------------------------------------------------------------ */
+/* batched solves: many independent tables, one persistent launch per  */
+/* sweep over all of them, captured in a CUDA graph.  The reference     */
+/* solves its targets one after another (Run.jl:1851-1958); this is the */
+/* same per-table solve_value!, run side by side.                       */
+/* ------------------------------------------------------------------ */
+
+typedef struct pg_batch pg_batch;
+
+typedef struct pg_batch_result {
+    int32_t tables;
+    int32_t converged;      /* tables whose last max-norm change <= tol      */
+    int32_t sweeps;         /* batched sweeps of the storage phase           */
+    int32_t polish_sweeps;  /* batched FP32 sweeps after a 16-bit phase      */
+    int32_t graph;          /* 1 when the sweeps ran as a CUDA graph         */
+    double kernel_ms;       /* device time of the batched sweeps             */
+    double elapsed_ms;      /* host wall time of the call                    */
+    int64_t cell_controls;  /* lookaheads of the tables' own sweeps          */
+} pg_batch_result;
+
+/* storage: PG_STORE_F32, F16 or BF16 for every table of the batch. */
+int pg_batch_create(pg_batch** out, int device, int32_t storage);
+int pg_batch_destroy(pg_batch* b);
+/* Add one table (arguments as pg_load_problem + its seeds); tile_rows > 0
+ * overrides the blend tiling (pg_set_tile_rows).  The table must run the
+ * plain scheme with the blend-then-shift sweep. */
+int pg_batch_add(pg_batch* b, const pg_grid6* g, const pg_model* m,
+                 const pg_params* p, const uint8_t* occ, const int64_t* tidx,
+                 int64_t ntidx, const float* ctl, int32_t nctl,
+                 int32_t tile_rows, int32_t* index);
+/* Seed every table and sweep them all, two Jacobi sweeps per step, until
+ * each table's max-norm change is <= tol or `iters` sweeps ran; then, for
+ * 16-bit storage, up to polish_sweeps FP32 sweeps of plain value iteration
+ * (target cells pinned) under the same rule. */
+int pg_batch_solve(pg_batch* b, int32_t iters, double tol,
+                   int32_t polish_sweeps, int32_t use_graph,
+                   pg_batch_result* res);
+/* Sweeps and last max-norm change of one table, and its context (owned by
+ * the batch; pg_get_value / pg_encode on it read the table). */
+int pg_batch_table(pg_batch* b, int32_t table, int32_t* sweeps,
+                   double* last_maxnorm, pg_ctx** ctx);
+
 /* ------------------------------------------------------------------ */
 /* adjoint: gradient of a loss on the converged table                  */
 /* ------------------------------------------------------------------ */

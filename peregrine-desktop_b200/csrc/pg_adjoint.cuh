@@ -232,16 +232,17 @@ __device__ __forceinline__ bool succ_corners(const GridT<float>& g, int64_t P, c
 }
 
 // Active cells: free, 0 < V < cap, policy admissible (mask bit) and the
-// policy's backup not clipped to the cap.  V plane-major FP32.
+// policy's backup not clipped to the cap.  V plane-major FP32.  Grid-stride
+// over the cells (the launch caps its grid).
 __global__ void k_adj_active(const float* __restrict__ V, const int16_t* __restrict__ pol,
                              const uint8_t* __restrict__ occ, const uint32_t* __restrict__ mask,
                              const uint32_t* __restrict__ recs, KParams kp,
                              uint8_t* __restrict__ active) {
-    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= kp.ncells) return;
     const Layout L = make_layout(kp);
     GridT<float> g;
     load_grid(g, kp.g);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < kp.ncells;
+         e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t pl = e / L.P;
     const int32_t r = (int32_t)(e - pl * L.P);
     const int32_t i = r / L.n[1], j = r - i * L.n[1];
@@ -277,21 +278,22 @@ __global__ void k_adj_active(const float* __restrict__ V, const int16_t* __restr
         }
     }
     active[e] = act;
+    }
 }
 
 // lambda_out += P^T lambda_in over the active cells (lambda_out holds c on
-// entry).  One thread per cell; 64 atomic adds per active cell with a
-// nonzero lambda.
+// entry).  Grid-stride over the cells; 64 atomic adds per active cell with
+// a nonzero lambda.
 __global__ void k_adj_scatter(const float* __restrict__ lam_in, float* __restrict__ lam_out,
                               const int16_t* __restrict__ pol, const uint8_t* __restrict__ active,
                               const uint32_t* __restrict__ recs, KParams kp) {
-    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= kp.ncells) return;
-    const float lv = lam_in[e];
-    if (lv == 0.0f || !active[e]) return;
     const Layout L = make_layout(kp);
     GridT<float> g;
     load_grid(g, kp.g);
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < kp.ncells;
+         e += (int64_t)gridDim.x * blockDim.x) {
+    const float lv = lam_in[e];
+    if (lv == 0.0f || !active[e]) continue;
     const int64_t pl = e / L.P;
     const int32_t r = (int32_t)(e - pl * L.P);
     const int32_t i = r / L.n[1], j = r - i * L.n[1];
@@ -304,7 +306,7 @@ __global__ void k_adj_scatter(const float* __restrict__ lam_in, float* __restric
     const uint32_t* rec = recs + ((size_t)pl * kp.nctl + u) * kURec;
     int32_t r0, c0;
     float tx, ty;
-    if (!succ_corners(g, L.P, rec, i, j, &r0, &c0, &tx, &ty)) return;
+    if (!succ_corners(g, L.P, rec, i, j, &r0, &c0, &tx, &ty)) continue;
     const int32_t r1 = min(r0 + 1, L.n[0] - 1), c1 = min(c0 + 1, L.n[1] - 1);
     const float wxy[4] = {(1.0f - tx) * (1.0f - ty), tx * (1.0f - ty), (1.0f - tx) * ty, tx * ty};
     const int32_t off[4] = {r0 * L.n[1] + c0, r1 * L.n[1] + c0, r0 * L.n[1] + c1, r1 * L.n[1] + c1};
@@ -315,6 +317,7 @@ __global__ void k_adj_scatter(const float* __restrict__ lam_in, float* __restric
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (wxy[q] != 0.0f) atomicAdd(dst + off[q], w * wxy[q]);
+    }
     }
 }
 

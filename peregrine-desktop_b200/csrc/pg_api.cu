@@ -902,6 +902,370 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
     return PG_OK;
 }
 
+int pg_set_tile_rows(pg_ctx* ctx, int32_t rows) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    pg::KParams& kp = ctx->kp;
+    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
+    if (rows < 1 || rows > n1 || (int64_t)rows * n2 > pg::kBMaxTileCells)
+        return fail(PG_EINVAL, "tile rows must be in [1, Nx] with rows * Ny <= 1024");
+    const int32_t nt = (n1 + rows - 1) / rows;
+    const int64_t need = kp.nplanes * nt;
+    if (need > ctx->nparts) {
+        double *ps = nullptr, *pm = nullptr;
+        PG_CUDA(cudaMalloc(&ps, sizeof(double) * need));
+        if (cudaMalloc(&pm, sizeof(double) * need) != cudaSuccess) {
+            cudaFree(ps);
+            return fail(PG_ENOMEM, "no room for the partials of that tiling");
+        }
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->part_sum);
+        cudaFree(ctx->part_max);
+        ctx->part_sum = ps;
+        ctx->part_max = pm;
+        ctx->nparts = need;
+    }
+    const int64_t cells = (int64_t)rows * n2;
+    int64_t th = 32 * (((cells + 2) / 3 + 31) / 32);
+    th = std::max<int64_t>(64, std::min<int64_t>(256, th));
+    kp.btile_x = rows;
+    kp.btiles_x = nt;
+    kp.bblock = (int32_t)th;
+    ctx->blend_ok = ctx->mask_ok && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
+    return PG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batched solves
+// ---------------------------------------------------------------------------
+
+struct pg_batch {
+    int device = 0;
+    int storage = PG_STORE_F32;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<pg_ctx*> tabs;
+    std::vector<std::vector<int64_t>> seeds;
+    std::vector<int32_t> sweeps;
+    std::vector<double> last_max;
+    pg::BatchTable* tabs_d = nullptr;
+    double* part_sum = nullptr;
+    double* part_max = nullptr;
+    double* out_d = nullptr;
+    double* out_h = nullptr;
+    int32_t* done_d = nullptr;
+    int32_t* done_h = nullptr;
+    int64_t cap_items = 0;
+    int cap_tabs = 0;
+
+    void free_bufs() {
+        if (tabs_d) cudaFree(tabs_d);
+        if (part_sum) cudaFree(part_sum);
+        if (part_max) cudaFree(part_max);
+        if (out_d) cudaFree(out_d);
+        if (out_h) cudaFreeHost(out_h);
+        if (done_d) cudaFree(done_d);
+        if (done_h) cudaFreeHost(done_h);
+        tabs_d = nullptr; part_sum = part_max = out_d = out_h = nullptr;
+        done_d = done_h = nullptr;
+        cap_items = 0;
+        cap_tabs = 0;
+    }
+};
+
+namespace {
+
+// Descriptors of every table at storage `st` (the V buffers of each
+// context, its masks and records); smem_out = the largest shared memory.
+int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, int64_t* nitems,
+                      size_t* smem_out) {
+    d.clear();
+    int64_t item = 0;
+    size_t smem = 0;
+    const int vn = 16 / (int)elem_bytes(st);
+    for (pg_ctx* c : b->tabs) {
+        pg::BatchTable t{};
+        t.V[0] = c->V[0];
+        t.V[1] = c->V[1];
+        t.occ = c->occ_d;
+        t.mask = c->mask_d;
+        t.recs = c->recs_d;
+        t.order = c->order_d;
+        t.kp = c->kp;
+        t.kp.tile_x = c->kp.btile_x;
+        t.kp.tiles_x = c->kp.btiles_x;
+        t.item0 = item;
+        t.nitems = c->kp.nplanes * c->kp.btiles_x;
+        t.vec = c->kp.g.n[1] % vn == 0 ? 1 : 0;
+        item += t.nitems;
+        smem = std::max(smem, pg::stencil_b_smem_bytes(c->kp));
+        d.push_back(t);
+    }
+    *nitems = item;
+    *smem_out = smem;
+    return PG_OK;
+}
+
+// Sweep every not-yet-converged table, two sweeps per step, until each has
+// a step whose second sweep moved no cell by more than tol, or max_sweeps.
+int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_graph,
+                double* kms, int32_t* steps_sweeps) {
+    std::vector<pg::BatchTable> d;
+    int64_t nitems = 0;
+    size_t smem = 0;
+    batch_descriptors(b, st, d, &nitems, &smem);
+    const int ntab = (int)b->tabs.size();
+    if (nitems > b->cap_items || ntab > b->cap_tabs) {
+        b->free_bufs();
+        PG_CUDA(cudaMalloc(&b->tabs_d, sizeof(pg::BatchTable) * ntab));
+        PG_CUDA(cudaMalloc(&b->part_sum, sizeof(double) * nitems));
+        PG_CUDA(cudaMalloc(&b->part_max, sizeof(double) * nitems));
+        PG_CUDA(cudaMalloc(&b->out_d, sizeof(double) * 2 * ntab));
+        PG_CUDA(cudaMallocHost(&b->out_h, sizeof(double) * 2 * ntab));
+        PG_CUDA(cudaMalloc(&b->done_d, sizeof(int32_t) * ntab));
+        PG_CUDA(cudaMallocHost(&b->done_h, sizeof(int32_t) * ntab));
+        b->cap_items = nitems;
+        b->cap_tabs = ntab;
+    }
+    PG_CUDA(cudaMemcpyAsync(b->tabs_d, d.data(), sizeof(pg::BatchTable) * ntab,
+                            cudaMemcpyHostToDevice, b->stream));
+    for (int t = 0; t < ntab; ++t) b->done_h[t] = 0;
+    PG_CUDA(cudaMemcpyAsync(b->done_d, b->done_h, sizeof(int32_t) * ntab, cudaMemcpyHostToDevice,
+                            b->stream));
+    int sms = 0;
+    PG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    const int per_sm = pg::batch_blocks_per_sm(st, smem);
+    if (per_sm <= 0) return fail(PG_EUNSUPPORTED, "the batched sweep does not fit on an SM");
+    const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * per_sm);
+
+    auto step = [&](cudaStream_t s) -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int parity = 0; parity < 2 && e == cudaSuccess; ++parity) {
+            e = pg::launch_stencil_b_batch(st, b->tabs_d, ntab, nitems, parity, b->done_d,
+                                           b->part_sum, b->part_max, smem, grid, s);
+            if (e == cudaSuccess)
+                e = pg::launch_reduce_batch(b->tabs_d, ntab, b->part_sum, b->part_max, b->out_d, s);
+        }
+        return e;
+    };
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (use_graph) {
+        PG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = step(b->stream);
+        cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return fail(PG_ECUDA, "graph capture of the batched sweep failed");
+        }
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return fail(PG_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+    }
+    int rc = PG_OK;
+    int32_t done_sw = 0;
+    while (done_sw < max_sweeps) {
+        cudaError_t e = cudaEventRecord(b->ev0, b->stream);
+        if (e == cudaSuccess) e = use_graph ? cudaGraphLaunch(exec, b->stream) : step(b->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->out_h, b->out_d, sizeof(double) * 2 * ntab,
+                                cudaMemcpyDeviceToHost, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        if (e != cudaSuccess) {
+            rc = fail(PG_ECUDA, std::string("batched sweep: ") + cudaGetErrorString(e));
+            break;
+        }
+        *kms += ms;
+        done_sw += 2;
+        int left = 0;
+        for (int t = 0; t < ntab; ++t) {
+            if (b->done_h[t]) continue;
+            b->sweeps[t] += 2;
+            b->last_max[t] = b->out_h[2 * t + 1];
+            if (b->last_max[t] <= tol) b->done_h[t] = 1;
+            else ++left;
+        }
+        if (!left) break;
+        e = cudaMemcpyAsync(b->done_d, b->done_h, sizeof(int32_t) * ntab, cudaMemcpyHostToDevice,
+                            b->stream);
+        if (e != cudaSuccess) {
+            rc = fail(PG_ECUDA, std::string("batched sweep: ") + cudaGetErrorString(e));
+            break;
+        }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    *steps_sweeps = done_sw;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pg_batch_create(pg_batch** out, int device, int32_t storage) {
+    if (!out) return fail(PG_EINVAL, "null output pointer");
+    if (storage != PG_STORE_F32 && storage != PG_STORE_F16 && storage != PG_STORE_BF16)
+        return fail(PG_EUNSUPPORTED, "batched solves store V in FP32, FP16 or BF16");
+    PG_CUDA(cudaSetDevice(device));
+    pg_batch* b = new pg_batch();
+    b->device = device;
+    b->storage = storage;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        delete b;
+        return fail(PG_ECUDA, "batch creation failed");
+    }
+    *out = b;
+    return PG_OK;
+}
+
+int pg_batch_destroy(pg_batch* b) {
+    if (!b) return PG_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    for (pg_ctx* c : b->tabs) pg_destroy(c);
+    b->free_bufs();
+    cudaEventDestroy(b->ev0);
+    cudaEventDestroy(b->ev1);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return PG_OK;
+}
+
+int pg_batch_add(pg_batch* b, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                 const uint8_t* occ, const int64_t* tidx, int64_t ntidx, const float* ctl,
+                 int32_t nctl, int32_t tile_rows, int32_t* index) {
+    if (!b) return fail(PG_EINVAL, "null batch");
+    if (ntidx < 0 || (ntidx > 0 && !tidx)) return fail(PG_EINVAL, "bad seed list");
+    pg_ctx* c = nullptr;
+    int rc = pg_create(&c, b->device);
+    if (rc) return rc;
+    rc = pg_load_problem(c, g, m, p, occ, ctl, nctl, b->storage);
+    if (!rc && !(c->stencil_ok && c->mask_ok && c->blend_ok))
+        rc = fail(PG_EUNSUPPORTED, "a batched table must run the blend-then-shift sweep (" +
+                                       (c->stencil_ok ? std::string("its records do not fit")
+                                                      : c->stencil_why) + ")");
+    if (!rc && tile_rows > 0) rc = pg_set_tile_rows(c, tile_rows);
+    for (int64_t t = 0; !rc && t < ntidx; ++t)
+        if (tidx[t] < 0 || tidx[t] >= c->kp.ncells)
+            rc = fail(PG_EINVAL, "seed index outside the grid");
+    if (rc) {
+        pg_destroy(c);
+        return rc;
+    }
+    b->tabs.push_back(c);
+    b->seeds.emplace_back(tidx, tidx + ntidx);
+    b->sweeps.push_back(0);
+    b->last_max.push_back(INFINITY);
+    if (index) *index = (int32_t)b->tabs.size() - 1;
+    return PG_OK;
+}
+
+int pg_batch_solve(pg_batch* b, int32_t iters, double tol, int32_t polish_sweeps,
+                   int32_t use_graph, pg_batch_result* res) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!b || b->tabs.empty()) return fail(PG_EINVAL, "empty batch");
+    PG_CUDA(cudaSetDevice(b->device));
+    const int ntab = (int)b->tabs.size();
+    // seed every table into V[0]
+    for (int t = 0; t < ntab; ++t) {
+        pg_ctx* c = b->tabs[t];
+        c->kp.relax = 0;
+        int rc = ensure_values(c, c->base_storage);
+        if (rc) return rc;
+        const int64_t nt = (int64_t)b->seeds[t].size();
+        if (nt > c->tidx_cap) {
+            if (c->tidx_d) cudaFree(c->tidx_d);
+            c->tidx_d = nullptr;
+            PG_CUDA(cudaMalloc(&c->tidx_d, sizeof(int64_t) * nt));
+            c->tidx_cap = nt;
+        }
+        if (nt > 0)
+            PG_CUDA(cudaMemcpyAsync(c->tidx_d, b->seeds[t].data(), sizeof(int64_t) * nt,
+                                    cudaMemcpyHostToDevice, c->stream));
+        c->ntidx = nt;
+        c->cur = 0;
+        cudaError_t e = pg::launch_fill_seed(c->storage, c->V[0], c->kp, c->tidx_d, nt, c->stream);
+        c->launches += 1;
+        if (e != cudaSuccess) return fail(PG_ECUDA, std::string("fill: ") + cudaGetErrorString(e));
+        PG_CUDA(cudaStreamSynchronize(c->stream));
+        b->sweeps[t] = 0;
+        b->last_max[t] = INFINITY;
+    }
+    double kms = 0.0;
+    int32_t sw = 0, psw = 0;
+    int rc = batch_phase(b, b->storage, iters, tol, use_graph != 0, &kms, &sw);
+    if (rc) return rc;
+    int32_t conv = 0;
+    for (int t = 0; t < ntab; ++t) conv += b->last_max[t] <= tol ? 1 : 0;
+    // 16-bit storage: continue every table in FP32 with plain value iteration
+    if (b->storage != PG_STORE_F32 && polish_sweeps > 0) {
+        for (int t = 0; t < ntab; ++t) {
+            pg_ctx* c = b->tabs[t];
+            const size_t bytes = (size_t)c->kp.ncells * 4;
+            void* nv[2] = {nullptr, nullptr};
+            PG_CUDA(cudaMalloc(&nv[0], bytes));
+            if (cudaMalloc(&nv[1], bytes) != cudaSuccess) {
+                cudaFree(nv[0]);
+                return fail(PG_ENOMEM, "no room for the FP32 polish buffers");
+            }
+            cudaError_t e = pg::launch_convert_to_f32(c->storage, c->V[0], (float*)nv[0],
+                                                      c->kp.ncells, c->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+            if (e != cudaSuccess) {
+                cudaFree(nv[0]);
+                cudaFree(nv[1]);
+                return fail(PG_ECUDA, "convert");
+            }
+            c->free_values();
+            c->V[0] = nv[0];
+            c->V[1] = nv[1];
+            c->cur = 0;
+            c->storage = PG_STORE_F32;
+            c->kp.relax = 1;
+        }
+        rc = batch_phase(b, PG_STORE_F32, polish_sweeps, tol, use_graph != 0, &kms, &psw);
+        for (pg_ctx* c : b->tabs) c->kp.relax = 0;
+        if (rc) return rc;
+        conv = 0;
+        for (int t = 0; t < ntab; ++t) conv += b->last_max[t] <= tol ? 1 : 0;
+    }
+    if (res) {
+        std::memset(res, 0, sizeof(*res));
+        res->tables = ntab;
+        res->converged = conv;
+        res->sweeps = sw;
+        res->polish_sweeps = psw;
+        res->graph = use_graph ? 1 : 0;
+        res->kernel_ms = kms;
+        int64_t cc = 0;
+        for (int t = 0; t < ntab; ++t)
+            cc += (int64_t)b->sweeps[t] * b->tabs[t]->kp.ncells * b->tabs[t]->kp.nctl;
+        res->cell_controls = cc;
+        res->elapsed_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return PG_OK;
+}
+
+int pg_batch_table(pg_batch* b, int32_t table, int32_t* sweeps, double* last_maxnorm,
+                   pg_ctx** ctx) {
+    if (!b || table < 0 || table >= (int32_t)b->tabs.size())
+        return fail(PG_EINVAL, "no such table in the batch");
+    if (sweeps) *sweeps = b->sweeps[table];
+    if (last_maxnorm) *last_maxnorm = b->last_max[table];
+    if (ctx) *ctx = b->tabs[table];
+    return PG_OK;
+}
+
 int pg_launch_count(pg_ctx* ctx, int64_t* launches) {
     if (!ctx || !launches) return fail(PG_EINVAL, "null argument");
     *launches = ctx->launches;

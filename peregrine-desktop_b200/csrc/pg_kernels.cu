@@ -67,9 +67,9 @@ __device__ __forceinline__ Layout make_layout(const KParams& kp) {
     return L;
 }
 
-// Deterministic block reduction of (sum, max) into per-block partials.
-__device__ __forceinline__ void block_partial(double s, double m, double* part_sum,
-                                              double* part_max) {
+// Deterministic block reduction of (sum, max) into partial slot `slot`.
+__device__ __forceinline__ void block_partial_at(double s, double m, double* part_sum,
+                                                 double* part_max, int64_t slot) {
     __shared__ double ws[32], wm[32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -88,8 +88,14 @@ __device__ __forceinline__ void block_partial(double s, double m, double* part_s
             s += __shfl_down_sync(0xffffffffu, s, o);
             m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
         }
-        if (lane == 0) { part_sum[blockIdx.x] = s; part_max[blockIdx.x] = m; }
+        if (lane == 0) { part_sum[slot] = s; part_max[slot] = m; }
     }
+}
+
+// ... into per-block partials.
+__device__ __forceinline__ void block_partial(double s, double m, double* part_sum,
+                                              double* part_max) {
+    block_partial_at(s, m, part_sum, part_max, blockIdx.x);
 }
 
 // One block sums the partials in a fixed order: thread t takes t, t+1024, ...
@@ -918,6 +924,59 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
     }
 #undef PG_SB
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t nitems,
+                                   int parity, const int32_t* done, double* part_sum,
+                                   double* part_max, size_t smem, int grid, cudaStream_t st) {
+#define PG_BB(S)                                                                                 \
+    {                                                                                            \
+        static bool attr_set = false;                                                            \
+        if (!attr_set) {                                                                         \
+            cudaError_t e = cudaFuncSetAttribute(k_stencil_b_batch<S>,                           \
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                                 200 * 1024);                                    \
+            if (e != cudaSuccess) return e;                                                      \
+            attr_set = true;                                                                     \
+        }                                                                                        \
+        k_stencil_b_batch<S><<<grid, 256, smem, st>>>(tabs, ntab, nitems, parity, done, part_sum, \
+                                                      part_max);                                 \
+        return cudaGetLastError();                                                               \
+    }
+    if (smem > 200 * 1024 || grid <= 0) return cudaErrorInvalidValue;
+    switch (storage) {
+        case PG_STORE_F32: PG_BB(float)
+        case PG_STORE_F16: PG_BB(__half)
+        case PG_STORE_BF16: PG_BB(__nv_bfloat16)
+    }
+#undef PG_BB
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_reduce_batch(const BatchTable* tabs, int ntab, const double* part_sum,
+                                const double* part_max, double* out, cudaStream_t st) {
+    k_reduce_batch<<<ntab, 256, 0, st>>>(tabs, part_sum, part_max, out);
+    return cudaGetLastError();
+}
+
+int batch_blocks_per_sm(int storage, size_t smem) {
+    int nb = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (storage) {
+        case PG_STORE_F32:
+            cudaFuncSetAttribute(k_stencil_b_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<float>, 256, smem);
+            break;
+        case PG_STORE_F16:
+            cudaFuncSetAttribute(k_stencil_b_batch<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__half>, 256, smem);
+            break;
+        case PG_STORE_BF16:
+            cudaFuncSetAttribute(k_stencil_b_batch<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__nv_bfloat16>, 256, smem);
+            break;
+    }
+    return e == cudaSuccess ? nb : 0;
 }
 
 size_t stencil_b_smem_bytes(const KParams& kp) {

@@ -88,17 +88,18 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Block = (plane, tile of kp.tile_x rows x all columns).  VEC: n2 is a
-// multiple of the 16-byte vector width, so window rows are whole vectors.
+// One work item = (plane, tile of kp.tile_x rows x all columns), item
+// number `item` of the table; its residual partial goes to slot `slot`.
+// VEC: n2 is a multiple of the 16-byte vector width, so window rows are
+// whole vectors.  Called by every thread of the block.
 template <typename S, bool ARGMIN, bool VEC>
-__global__ void __launch_bounds__(256)
-    k_stencil_b(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
-                const uint32_t* __restrict__ mask, const uint32_t* __restrict__ recs, KParams kp,
-                const int32_t* __restrict__ order, double* part_sum, double* part_max,
-                int16_t* argmin) {
+__device__ __forceinline__ void stencil_b_item(
+    const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
+    const uint32_t* __restrict__ mask, const uint32_t* __restrict__ recs, const KParams& kp,
+    const int32_t* __restrict__ order, double* part_sum, double* part_max, int16_t* argmin,
+    int64_t item, int64_t slot, unsigned char* smem_raw) {
     typedef Ar<float> R_;
     constexpr int VN = BVec<S>::N;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nctl = kp.nctl;
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], W = mask_words(n2);
     const int32_t TX = kp.tile_x;
@@ -115,8 +116,8 @@ __global__ void __launch_bounds__(256)
     load_grid(g, kp.g);
     const float cap = kp.p.cap;
     const int64_t P = L.P;
-    const int64_t pl = blockIdx.x / kp.tiles_x;
-    const int32_t xt = (int32_t)(blockIdx.x - pl * kp.tiles_x);
+    const int64_t pl = item / kp.tiles_x;
+    const int32_t xt = (int32_t)(item - pl * kp.tiles_x);
     const int32_t x0 = xt * TX;
     const int32_t nr = min(TX, n1 - x0);
     const int32_t ncell = nr * n2;
@@ -324,5 +325,79 @@ __global__ void __launch_bounds__(256)
             Vo0[e] = ov;
         }
     }
-    block_partial(dsum, dmax, part_sum, part_max);
+    block_partial_at(dsum, dmax, part_sum, part_max, slot);
+}
+
+// The single-table sweep: one block per work item.
+template <typename S, bool ARGMIN, bool VEC>
+__global__ void __launch_bounds__(256)
+    k_stencil_b(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
+                const uint32_t* __restrict__ mask, const uint32_t* __restrict__ recs, KParams kp,
+                const int32_t* __restrict__ order, double* part_sum, double* part_max,
+                int16_t* argmin) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    stencil_b_item<S, ARGMIN, VEC>(Vin, Vout, occ, mask, recs, kp, order, part_sum, part_max,
+                                   argmin, blockIdx.x, blockIdx.x, smem_raw);
+}
+
+// Many tables in one launch (BatchTable, pg_types.h).  Work items of all
+// tables are numbered contiguously (table t owns items [item0, item0 +
+// nitems)); a persistent grid walks them, and items of a table whose `done`
+// flag is set only clear their residual slot.  The two value buffers of a
+// table alternate with `parity`.
+
+template <typename S>
+__global__ void __launch_bounds__(256)
+    k_stencil_b_batch(const BatchTable* __restrict__ tabs, int ntab, int64_t nitems, int parity,
+                      const int32_t* __restrict__ done, double* part_sum, double* part_max) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        int lo = 0, hi = ntab - 1;  // the table owning item `it`
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tabs[mid].item0 <= it) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchTable& tb = tabs[lo];
+        __syncthreads();  // the previous item's shared memory is free
+        if (done[lo]) {
+            if (threadIdx.x == 0) { part_sum[it] = 0.0; part_max[it] = 0.0; }
+            continue;
+        }
+        const S* vin = static_cast<const S*>(tb.V[parity]);
+        S* vout = const_cast<S*>(static_cast<const S*>(tb.V[1 - parity]));
+        if (tb.vec)
+            stencil_b_item<S, false, true>(vin, vout, tb.occ, tb.mask, tb.recs, tb.kp, tb.order,
+                                           part_sum, part_max, nullptr, it - tb.item0, it, smem_raw);
+        else
+            stencil_b_item<S, false, false>(vin, vout, tb.occ, tb.mask, tb.recs, tb.kp, tb.order,
+                                            part_sum, part_max, nullptr, it - tb.item0, it, smem_raw);
+    }
+}
+
+// Per-table (sum, max) of the residual partials: block t reduces table t's
+// slots in a fixed order into out[2t], out[2t+1].
+__global__ void k_reduce_batch(const BatchTable* __restrict__ tabs, const double* part_sum,
+                               const double* part_max, double* out) {
+    __shared__ double ss[256], sm[256];
+    const BatchTable& tb = tabs[blockIdx.x];
+    double s = 0.0, m = 0.0;
+    for (int64_t i = threadIdx.x; i < tb.nitems; i += blockDim.x) {
+        s += part_sum[tb.item0 + i];
+        m = fmax(m, part_max[tb.item0 + i]);
+    }
+    ss[threadIdx.x] = s;
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            ss[threadIdx.x] += ss[threadIdx.x + w];
+            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * blockIdx.x] = ss[0];
+        out[2 * blockIdx.x + 1] = sm[0];
+    }
 }

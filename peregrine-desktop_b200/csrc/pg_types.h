@@ -54,6 +54,20 @@ struct SweepBufs {
     double* out;  // [2]: L1 total, max-norm
 };
 
+// One table of a batched sweep: its buffers, its work items in the batch's
+// numbering and its kernel parameters (tile_x / tiles_x = the blend tiling).
+struct BatchTable {
+    const void* V[2];
+    const uint8_t* occ;
+    const uint32_t* mask;
+    const uint32_t* recs;
+    const int32_t* order;
+    int64_t item0, nitems;
+    int32_t vec;
+    int32_t pad;
+    KParams kp;
+};
+
 // Records msg as the text pg_last_error returns on this thread; returns code.
 int set_last_error(int code, const std::string& msg);
 

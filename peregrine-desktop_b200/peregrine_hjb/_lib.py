@@ -31,7 +31,9 @@ EXPORTS = (
     "pg_abi_version", "pg_last_error", "pg_default_opts", "pg_create", "pg_destroy",
     "pg_solve_value", "pg_load_problem", "pg_solve", "pg_get_value", "pg_set_value",
     "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
-    "pg_launch_count", "pg_adjoint", "pg_measure_peaks", "pg_sweep_noalloc",
+    "pg_launch_count", "pg_set_tile_rows", "pg_batch_create", "pg_batch_destroy",
+    "pg_batch_add", "pg_batch_solve", "pg_batch_table", "pg_adjoint", "pg_measure_peaks",
+    "pg_sweep_noalloc",
 )
 
 
@@ -73,6 +75,12 @@ class SolveResult(C.Structure):
                 ("last_delta", C.c_double), ("last_maxnorm", C.c_double),
                 ("kernel_ms", C.c_double), ("elapsed_ms", C.c_double),
                 ("cell_controls", C.c_int64)]
+
+
+class BatchResult(C.Structure):
+    _fields_ = [("tables", C.c_int32), ("converged", C.c_int32), ("sweeps", C.c_int32),
+                ("polish_sweeps", C.c_int32), ("graph", C.c_int32), ("kernel_ms", C.c_double),
+                ("elapsed_ms", C.c_double), ("cell_controls", C.c_int64)]
 
 
 class AdjointResult(C.Structure):
@@ -119,6 +127,13 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "pg_encode": (C.c_int, [vp, i32, f64, f64, i64, i64, vp, P(i64), P(i64)]),
         "pg_time_sweeps": (C.c_int, [vp, i32, i32, i32, P(f64)]),
         "pg_launch_count": (C.c_int, [vp, P(i64)]),
+        "pg_set_tile_rows": (C.c_int, [vp, i32]),
+        "pg_batch_create": (C.c_int, [P(vp), C.c_int, i32]),
+        "pg_batch_destroy": (C.c_int, [vp]),
+        "pg_batch_add": (C.c_int, [vp, P(Grid6), P(Model), P(Params), vp, vp, i64, vp, i32, i32,
+                                   P(i32)]),
+        "pg_batch_solve": (C.c_int, [vp, i32, f64, i32, i32, P(BatchResult)]),
+        "pg_batch_table": (C.c_int, [vp, i32, P(i32), P(f64), P(vp)]),
         "pg_adjoint": (C.c_int, [vp, vp, i32, i32, f64, vp, P(AdjointResult)]),
         "pg_measure_peaks": (C.c_int, [C.c_int, P(f64), P(f64), P(f64)]),
         "pg_sweep_noalloc": (C.c_int, [P(Grid6), P(Model), P(Params), vp, vp, i32, vp, vp, i32,
@@ -273,6 +288,9 @@ class Context:
                                     C.byref(res)))
         return grad, res
 
+    def set_tile_rows(self, rows: int) -> None:
+        _check(self._lib.pg_set_tile_rows(self._h, int(rows)))
+
     def launch_count(self) -> int:
         n = C.c_int64()
         _check(self._lib.pg_launch_count(self._h, C.byref(n)))
@@ -286,6 +304,65 @@ def measure_peaks(device: int = 0) -> dict:
     s, l2, f = C.c_double(), C.c_double(), C.c_double()
     _check(lib.pg_measure_peaks(int(device), C.byref(s), C.byref(l2), C.byref(f)))
     return {"smem_gbs": s.value, "l2_gbs": l2.value, "fma_tflops": f.value}
+
+
+class Batch:
+    """Many independent tables solved side by side (pg_batch_*)."""
+
+    def __init__(self, device: int = 0, storage: str = "fp16"):
+        self._lib = load_library()
+        h = C.c_void_p()
+        _check(self._lib.pg_batch_create(C.byref(h), int(device), STORAGES[storage]))
+        self._h = h
+        self.ncells = []
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.pg_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, grid: Grid6, model: Model, params: Params, occ: np.ndarray, seeds: np.ndarray,
+            ctl: np.ndarray, tile_rows: int = 0) -> int:
+        occ = np.ascontiguousarray(occ, dtype=np.uint8)
+        seeds = np.ascontiguousarray(seeds, dtype=np.int64)
+        ctl = np.ascontiguousarray(ctl, dtype=np.float32)
+        idx = C.c_int32()
+        _check(self._lib.pg_batch_add(self._h, C.byref(grid), C.byref(model), C.byref(params),
+                                      _ptr(occ), _ptr(seeds), seeds.size, _ptr(ctl),
+                                      ctl.size // 3, int(tile_rows), C.byref(idx)))
+        self.ncells.append(int(np.prod(np.array([int(v) for v in grid.n], dtype=np.int64))))
+        return idx.value
+
+    def solve(self, iters: int, tol: float, polish_sweeps: int = 0, graph: bool = True):
+        res = BatchResult()
+        _check(self._lib.pg_batch_solve(self._h, int(iters), float(tol), int(polish_sweeps),
+                                        1 if graph else 0, C.byref(res)))
+        return res
+
+    def table(self, t: int):
+        """(sweeps, last max-norm change) of table t."""
+        sw, mx = C.c_int32(), C.c_double()
+        _check(self._lib.pg_batch_table(self._h, int(t), C.byref(sw), C.byref(mx), None))
+        return sw.value, mx.value
+
+    def get_value(self, t: int) -> np.ndarray:
+        ctx = C.c_void_p()
+        _check(self._lib.pg_batch_table(self._h, int(t), None, None, C.byref(ctx)))
+        out = np.empty(self.ncells[t], dtype=np.float32)
+        _check(self._lib.pg_get_value(ctx, _ptr(out)))
+        return out
 
 
 def sweep_noalloc(grid: Grid6, model: Model, params: Params, occ_dev: int, ctl_dev: int,

@@ -81,6 +81,32 @@ def test_adjoint_matches_central_differences(setup):
         assert abs(s["g"][k] - fd) <= bound, (name, s["g"][k], fd)
 
 
+def test_adjoint_on_more_cells_than_one_launch_wave(og):
+    """24x24x8x9x9x9 = 3.4M cells: more than one pass of a capped grid, so
+    every cell-parallel kernel of the adjoint must cover the whole table."""
+    pr = Problem("tiny", seed=7, n=(24, 24, 8, 9, 9, 9))
+    spec = ag.SolveSpec.from_problem(pr, iters=6000, tol=1e-6)
+    th0 = ag.theta_of(spec.model)
+    states = ag.start_states(spec.grid, pr.occ, 1024, seed=2)
+    idx, w = ag.interp_weights(spec.grid, states)
+    c = np.zeros(pr.ncells, np.float64)
+    np.add.at(c, idx.ravel(), (w / len(states)).ravel())
+    V, _, ctx = ag.solve(spec, th0, keep=True)
+    try:
+        g, ares = ctx.adjoint(c.astype(np.float32))
+        _, _, pol = ctx.sweep(phase=0, kernel=_lib.KERNEL_STENCIL, argmin=True)
+    finally:
+        ctx.close()
+    g_ = og.copy_struct(spec.grid, og.OGrid)
+    m_ = og.copy_struct(spec.model, og.OModel)
+    p_ = og.copy_struct(spec.params, og.OParams)
+    g_ref, _, nact = og.adjoint_grad_f64(V.astype(np.float64), pol, pr.occ, g_, m_, pr.ctl, p_, c,
+                                         iters=20000, tol=1e-9)
+    assert abs(nact - ares.active_cells) <= 0.001 * nact
+    err = np.abs(g - g_ref) / np.max(np.abs(g_ref))
+    assert err.max() <= REF_TOL, dict(zip(ag.THETA_NAMES, err))
+
+
 def test_autograd_function_matches_the_direct_call(setup):
     s = setup
     theta = torch.tensor(s["th0"], requires_grad=True)
