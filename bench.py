@@ -353,45 +353,47 @@ def run_ours(args, rank, world, local_rank):
 
 
 def run_accuracy(args, local_rank):
-    """Time-to-converge and precision report: the same table solved to the
-    max-norm stop (1e-4 s) with FP32 storage, FP64 (the device oracle), and
-    FP16 / BF16 storage followed by FP32 polish sweeps; errors of each against
-    FP64 and FP32."""
+    """Time-to-converge at <= 2 ms max error: the table solved with FP32
+    storage and with 16-bit storages (FP16, BF16, Q16 fixed point) followed by
+    FP32 polish sweeps, each to a ladder of max-norm stop tolerances; the
+    error of every result against the FP64 table converged to 1e-9 s; the
+    device time of the cheapest run within 2 ms, per storage."""
     import numpy as np
     import torch
     from peregrine_hjb import _lib
 
     torch.cuda.set_device(local_rank)
     pr = problem_for_rank(0)
-    args_c = (pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.seeds, pr.ctl,
-              args.max_sweeps, 1e-4)
-    runs = {}
-    tables = {}
-    for name, kw in (("fp32", dict(storage="fp32")), ("fp64", dict(storage="fp64")),
-                     ("fp16", dict(storage="fp16", polish_sweeps=args.max_sweeps)),
-                     ("bf16", dict(storage="bf16", polish_sweeps=args.max_sweeps))):
-        if name not in args.storages.split(","):
-            continue
-        opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL, **kw)
-        V, res = _lib.solve_value(*args_c, opts, device=local_rank)
-        tables[name] = V
-        runs[name] = {"sweeps": res.iterations, "polish_sweeps": res.polish_iterations,
-                      "kernel_s": res.kernel_ms / 1000.0, "wall_s": res.elapsed_ms / 1000.0,
-                      "last_maxnorm": res.last_maxnorm}
-    ref = tables.get("fp64", tables.get("fp32"))
-    reached = ref < np.float32(pr.params.cap) - 1e-3
-    for name, V in tables.items():
-        d = np.abs(V.astype(np.float64) - ref.astype(np.float64))
-        runs[name]["max_abs_err_vs_" + ("fp64" if "fp64" in tables else "fp32")] = float(d.max())
-        runs[name]["rms_err_reached"] = float(np.sqrt(np.mean(d[reached] ** 2))) if reached.any() else 0.0
-        if "fp32" in tables and name != "fp32":
-            runs[name]["max_abs_err_vs_fp32"] = float(np.max(np.abs(V - tables["fp32"])))
-    line = {"report": "accuracy", "workload": WORKLOAD, "cells": pr.ncells, "controls": pr.nctl,
-            "stop": "max-norm residual < 1e-4 s", "runs": runs}
-    if "fp32" in runs:
-        for name in ("fp16", "bf16"):
-            if name in runs:
-                runs[name]["speedup_vs_fp32"] = runs["fp32"]["kernel_s"] / runs[name]["kernel_s"]
+    base = (pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.seeds, pr.ctl)
+    ropts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL,
+                              storage="fp64")
+    ref, rres = _lib.solve_value(*base, 20000, 1e-9, ropts, device=local_rank)
+    ref = ref.astype(np.float64)
+    reached = (ref > 0) & (ref < float(pr.params.cap) - 1e-3)
+    target = 2e-3
+    runs, ttc = {}, {}
+    for name in args.storages.split(","):
+        runs[name] = []
+        for tol in (1e-4, 3e-5, 1e-5, 3e-6):
+            kw = dict(storage=name)
+            if name != "fp32":
+                kw["polish_sweeps"] = args.max_sweeps
+            opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL, **kw)
+            V, res = _lib.solve_value(*base, args.max_sweeps, tol, opts, device=local_rank)
+            err = np.abs(V.astype(np.float64) - ref)[reached]
+            runs[name].append({"tol": tol, "sweeps": res.iterations - res.polish_iterations,
+                               "polish_sweeps": res.polish_iterations,
+                               "kernel_s": res.kernel_ms / 1000.0,
+                               "max_err": float(err.max()), "rms_err": float(np.sqrt(np.mean(err ** 2)))})
+        ok = [r["kernel_s"] for r in runs[name] if r["max_err"] <= target]
+        ttc[name] = min(ok) if ok else None
+    line = {"report": "time_to_converge", "workload": WORKLOAD, "cells": pr.ncells,
+            "controls": pr.nctl, "target_max_err_s": target,
+            "reference": {"storage": "fp64", "stop": "max-norm < 1e-9 s", "sweeps": rres.iterations},
+            "error_over": "reached cells (0 < V < cap) against the reference",
+            "runs": runs, "time_to_converge_s": ttc}
+    if ttc.get("fp32"):
+        line["speedup_vs_fp32"] = {k: (ttc["fp32"] / v if v else None) for k, v in ttc.items()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -411,7 +413,7 @@ def main():
     ap.add_argument("--accuracy", action="store_true",
                     help="time-to-converge and FP32/FP64/FP16/BF16 error report instead of "
                          "the throughput line")
-    ap.add_argument("--storages", default="fp32,fp64,fp16,bf16")
+    ap.add_argument("--storages", default="fp32,fp16,bf16,q16")
     ap.add_argument("--max-sweeps", type=int, default=4000)
     args = ap.parse_args()
     globals()["WORKLOAD"] = args.workload

@@ -95,6 +95,10 @@ typedef struct pg_params {
 #define PG_STORE_F16  1
 #define PG_STORE_BF16 2
 #define PG_STORE_F64  3
+/* Q16: unsigned 16-bit fixed point, V = code * 2^-11 s (0.49 ms steps,
+ * 0..32 s; value_cap must be below 32 s).  Swept by the blend-then-shift
+ * kernel only; a 16-bit storage like F16/BF16, with the FP32 polish. */
+#define PG_STORE_Q16  4
 
 /* Sweep kernel selection. */
 #define PG_KERNEL_AUTO     0  /* stencil when the scheme allows it, else cellform */

@@ -41,6 +41,7 @@ size_t elem_bytes(int storage) {
         case PG_STORE_F32: return 4;
         case PG_STORE_F16: return 2;
         case PG_STORE_BF16: return 2;
+        case PG_STORE_Q16: return 2;
         case PG_STORE_F64: return 8;
     }
     return 0;
@@ -195,6 +196,9 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
     const void* vin = ctx->V[ctx->cur];
     void* vout = ctx->V[1 - ctx->cur];
     cudaError_t e;
+    if (ctx->storage == PG_STORE_Q16 &&
+        (esc || kernel != PG_KERNEL_STENCIL || !ctx->mask_ok || !ctx->blend_ok))
+        return fail(PG_EUNSUPPORTED, "Q16 storage is swept by the blend-then-shift kernel only");
     if (esc || kernel == PG_KERNEL_CELLFORM)
         e = pg::launch_cellform(ctx->storage, esc, vin, vout, ctx->occ_d,
                                 use_pol ? ctx->pol_d : nullptr, ctx->kp, ctx->ctl_d, sb, argmin_d,
@@ -357,6 +361,8 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     if (nctl < 2 || nctl > 32767)
         return fail(PG_EINVAL, "the control table needs coast plus at least one command");
     if (elem_bytes(storage) == 0) return fail(PG_EINVAL, "unknown storage");
+    if (storage == PG_STORE_Q16 && !(p->cap < 32.0f))
+        return fail(PG_EUNSUPPORTED, "Q16 storage holds values below 32 s; value_cap is larger");
     if (!(p->cap > 0.0f)) return fail(PG_EINVAL, "value_cap must be positive");
     if (p->nsub < 1) return fail(PG_EINVAL, "substeps must be >= 1");
     if (p->checks < 1) return fail(PG_EINVAL, "sweep_checks must be >= 1");
@@ -570,7 +576,8 @@ int pg_solve(pg_ctx* ctx, const int64_t* tidx, int64_t ntidx, int32_t iters, dou
 
     // 16-bit storage: continue in FP32 from the converged 16-bit table until
     // the same stop rule holds at FP32 resolution.
-    if ((ctx->storage == PG_STORE_F16 || ctx->storage == PG_STORE_BF16) && opts.polish_sweeps > 0) {
+    if ((ctx->storage == PG_STORE_F16 || ctx->storage == PG_STORE_BF16 ||
+         ctx->storage == PG_STORE_Q16) && opts.polish_sweeps > 0) {
         const size_t bytes = (size_t)ctx->kp.ncells * 4;
         void* nv[2] = {nullptr, nullptr};
         PG_CUDA(cudaMalloc(&nv[0], bytes));
@@ -1039,12 +1046,15 @@ int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_gr
     const int per_sm = pg::batch_blocks_per_sm(st, smem);
     if (per_sm <= 0) return fail(PG_EUNSUPPORTED, "the batched sweep does not fit on an SM");
     const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * per_sm);
+    bool any_vec = false, any_scalar = false;
+    for (const auto& t : d) (t.vec ? any_vec : any_scalar) = true;
 
     auto step = [&](cudaStream_t s) -> cudaError_t {
         cudaError_t e = cudaSuccess;
         for (int parity = 0; parity < 2 && e == cudaSuccess; ++parity) {
             e = pg::launch_stencil_b_batch(st, b->tabs_d, ntab, nitems, parity, b->done_d,
-                                           b->part_sum, b->part_max, smem, grid, s);
+                                           b->part_sum, b->part_max, smem, grid, any_vec,
+                                           any_scalar, s);
             if (e == cudaSuccess)
                 e = pg::launch_reduce_batch(b->tabs_d, ntab, b->part_sum, b->part_max, b->out_d, s);
         }
@@ -1112,8 +1122,9 @@ extern "C" {
 
 int pg_batch_create(pg_batch** out, int device, int32_t storage) {
     if (!out) return fail(PG_EINVAL, "null output pointer");
-    if (storage != PG_STORE_F32 && storage != PG_STORE_F16 && storage != PG_STORE_BF16)
-        return fail(PG_EUNSUPPORTED, "batched solves store V in FP32, FP16 or BF16");
+    if (storage != PG_STORE_F32 && storage != PG_STORE_F16 && storage != PG_STORE_BF16 &&
+        storage != PG_STORE_Q16)
+        return fail(PG_EUNSUPPORTED, "batched solves store V in FP32, FP16, BF16 or Q16");
     PG_CUDA(cudaSetDevice(device));
     pg_batch* b = new pg_batch();
     b->device = device;

@@ -54,6 +54,21 @@ template <> struct Conv<__nv_bfloat16> {
         return __float2bfloat16_rn((float)v);
     }
 };
+// Q16: V = u * 2^-11 s, u rounded to nearest and saturated to [0, 65535]
+// (0 .. 32 s, a uniform 0.49 ms quantum; the conversions are exact scalings).
+template <> struct Conv<Q16> {
+    static __device__ __forceinline__ float ld(const Q16* p) {
+        return (float)__ldg(&p->u) * kQ16Step;
+    }
+    static __device__ __forceinline__ float val(Q16 v) { return (float)v.u * kQ16Step; }
+    template <typename T> static __device__ __forceinline__ Q16 st(T v) {
+        float f = rintf((float)v * kQ16Scale);
+        f = f >= 0.0f ? fminf(f, 65535.0f) : (f < 0.0f ? 0.0f : 65535.0f);
+        Q16 q;
+        q.u = (uint16_t)f;
+        return q;
+    }
+};
 
 // ---------------------------------------------------------------------------
 // small utilities
@@ -652,6 +667,7 @@ cudaError_t launch_fill_seed(int storage, void* V, const KParams& kp, const int6
         case PG_STORE_F32: return fill_seed_t<float>(V, kp, tidx_dev, nt, st);
         case PG_STORE_F16: return fill_seed_t<__half>(V, kp, tidx_dev, nt, st);
         case PG_STORE_BF16: return fill_seed_t<__nv_bfloat16>(V, kp, tidx_dev, nt, st);
+        case PG_STORE_Q16: return fill_seed_t<Q16>(V, kp, tidx_dev, nt, st);
         case PG_STORE_F64: return fill_seed_t<double>(V, kp, tidx_dev, nt, st);
     }
     return cudaErrorInvalidValue;
@@ -664,6 +680,7 @@ cudaError_t launch_seed_only(int storage, void* V, const KParams& kp, const int6
         case PG_STORE_F32: k_seed<float><<<grid_for(nt, 256), 256, 0, st>>>((float*)V, tidx_dev, nt, kp); break;
         case PG_STORE_F16: k_seed<__half><<<grid_for(nt, 256), 256, 0, st>>>((__half*)V, tidx_dev, nt, kp); break;
         case PG_STORE_BF16: k_seed<__nv_bfloat16><<<grid_for(nt, 256), 256, 0, st>>>((__nv_bfloat16*)V, tidx_dev, nt, kp); break;
+        case PG_STORE_Q16: k_seed<Q16><<<grid_for(nt, 256), 256, 0, st>>>((Q16*)V, tidx_dev, nt, kp); break;
         case PG_STORE_F64: k_seed<double><<<grid_for(nt, 256), 256, 0, st>>>((double*)V, tidx_dev, nt, kp); break;
         default: return cudaErrorInvalidValue;
     }
@@ -677,6 +694,7 @@ cudaError_t launch_to_rowmajor(int storage, const void* V, float* out, const KPa
         case PG_STORE_F32: k_to_rowmajor<float><<<b, 256, 0, st>>>((const float*)V, out, kp); break;
         case PG_STORE_F16: k_to_rowmajor<__half><<<b, 256, 0, st>>>((const __half*)V, out, kp); break;
         case PG_STORE_BF16: k_to_rowmajor<__nv_bfloat16><<<b, 256, 0, st>>>((const __nv_bfloat16*)V, out, kp); break;
+        case PG_STORE_Q16: k_to_rowmajor<Q16><<<b, 256, 0, st>>>((const Q16*)V, out, kp); break;
         case PG_STORE_F64: k_to_rowmajor<double><<<b, 256, 0, st>>>((const double*)V, out, kp); break;
         default: return cudaErrorInvalidValue;
     }
@@ -690,6 +708,7 @@ cudaError_t launch_from_rowmajor(int storage, const float* in, void* V, const KP
         case PG_STORE_F32: k_from_rowmajor<float><<<b, 256, 0, st>>>(in, (float*)V, kp); break;
         case PG_STORE_F16: k_from_rowmajor<__half><<<b, 256, 0, st>>>(in, (__half*)V, kp); break;
         case PG_STORE_BF16: k_from_rowmajor<__nv_bfloat16><<<b, 256, 0, st>>>(in, (__nv_bfloat16*)V, kp); break;
+        case PG_STORE_Q16: k_from_rowmajor<Q16><<<b, 256, 0, st>>>(in, (Q16*)V, kp); break;
         case PG_STORE_F64: k_from_rowmajor<double><<<b, 256, 0, st>>>(in, (double*)V, kp); break;
         default: return cudaErrorInvalidValue;
     }
@@ -702,6 +721,7 @@ cudaError_t launch_convert_to_f32(int storage, const void* in, float* out, int64
     switch (storage) {
         case PG_STORE_F16: k_convert<__half, float><<<b, 256, 0, st>>>((const __half*)in, out, n); break;
         case PG_STORE_BF16: k_convert<__nv_bfloat16, float><<<b, 256, 0, st>>>((const __nv_bfloat16*)in, out, n); break;
+        case PG_STORE_Q16: k_convert<Q16, float><<<b, 256, 0, st>>>((const Q16*)in, out, n); break;
         case PG_STORE_F32: return cudaMemcpyAsync(out, in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
         default: return cudaErrorInvalidValue;
     }
@@ -921,6 +941,7 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
         case PG_STORE_F32: PG_SB(float);
         case PG_STORE_F16: PG_SB(__half);
         case PG_STORE_BF16: PG_SB(__nv_bfloat16);
+        case PG_STORE_Q16: PG_SB(Q16);
     }
 #undef PG_SB
     return cudaErrorInvalidValue;
@@ -928,19 +949,27 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
 
 cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t nitems,
                                    int parity, const int32_t* done, double* part_sum,
-                                   double* part_max, size_t smem, int grid, cudaStream_t st) {
+                                   double* part_max, size_t smem, int grid, bool any_vec,
+                                   bool any_scalar, cudaStream_t st) {
 #define PG_BB(S)                                                                                 \
     {                                                                                            \
         static bool attr_set = false;                                                            \
         if (!attr_set) {                                                                         \
-            cudaError_t e = cudaFuncSetAttribute(k_stencil_b_batch<S>,                           \
+            cudaError_t e = cudaFuncSetAttribute(k_stencil_b_batch<S, true>,                     \
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                                  200 * 1024);                                    \
+            if (e == cudaSuccess)                                                                \
+                e = cudaFuncSetAttribute(k_stencil_b_batch<S, false>,                            \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
             if (e != cudaSuccess) return e;                                                      \
             attr_set = true;                                                                     \
         }                                                                                        \
-        k_stencil_b_batch<S><<<grid, 256, smem, st>>>(tabs, ntab, nitems, parity, done, part_sum, \
-                                                      part_max);                                 \
+        if (any_vec)                                                                             \
+            k_stencil_b_batch<S, true><<<grid, 256, smem, st>>>(tabs, ntab, nitems, parity, done, \
+                                                                part_sum, part_max);             \
+        if (any_scalar)                                                                          \
+            k_stencil_b_batch<S, false><<<grid, 256, smem, st>>>(tabs, ntab, nitems, parity,     \
+                                                                 done, part_sum, part_max);      \
         return cudaGetLastError();                                                               \
     }
     if (smem > 200 * 1024 || grid <= 0) return cudaErrorInvalidValue;
@@ -948,6 +977,7 @@ cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab
         case PG_STORE_F32: PG_BB(float)
         case PG_STORE_F16: PG_BB(__half)
         case PG_STORE_BF16: PG_BB(__nv_bfloat16)
+        case PG_STORE_Q16: PG_BB(Q16)
     }
 #undef PG_BB
     return cudaErrorInvalidValue;
@@ -964,16 +994,20 @@ int batch_blocks_per_sm(int storage, size_t smem) {
     cudaError_t e = cudaErrorInvalidValue;
     switch (storage) {
         case PG_STORE_F32:
-            cudaFuncSetAttribute(k_stencil_b_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<float>, 256, smem);
+            cudaFuncSetAttribute(k_stencil_b_batch<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<float, true>, 256, smem);
             break;
         case PG_STORE_F16:
-            cudaFuncSetAttribute(k_stencil_b_batch<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__half>, 256, smem);
+            cudaFuncSetAttribute(k_stencil_b_batch<__half, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__half, true>, 256, smem);
             break;
         case PG_STORE_BF16:
-            cudaFuncSetAttribute(k_stencil_b_batch<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__nv_bfloat16>, 256, smem);
+            cudaFuncSetAttribute(k_stencil_b_batch<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__nv_bfloat16, true>, 256, smem);
+            break;
+        case PG_STORE_Q16:
+            cudaFuncSetAttribute(k_stencil_b_batch<Q16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<Q16, true>, 256, smem);
             break;
     }
     return e == cudaSuccess ? nb : 0;
@@ -1045,6 +1079,7 @@ cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t
         case PG_STORE_F32: k_encode<float><<<b, 256, 0, st>>>((const float*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
         case PG_STORE_F16: k_encode<__half><<<b, 256, 0, st>>>((const __half*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
         case PG_STORE_BF16: k_encode<__nv_bfloat16><<<b, 256, 0, st>>>((const __nv_bfloat16*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
+        case PG_STORE_Q16: k_encode<Q16><<<b, 256, 0, st>>>((const Q16*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
         case PG_STORE_F64: k_encode<double><<<b, 256, 0, st>>>((const double*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
         default: return cudaErrorInvalidValue;
     }

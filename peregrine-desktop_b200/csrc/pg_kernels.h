@@ -47,7 +47,8 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
 size_t stencil_b_smem_bytes(const KParams& kp);
 cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t nitems,
                                    int parity, const int32_t* done, double* part_sum,
-                                   double* part_max, size_t smem, int grid, cudaStream_t st);
+                                   double* part_max, size_t smem, int grid, bool any_vec,
+                                   bool any_scalar, cudaStream_t st);
 cudaError_t launch_reduce_batch(const BatchTable* tabs, int ntab, const double* part_sum,
                                 const double* part_max, double* out, cudaStream_t st);
 int batch_blocks_per_sm(int storage, size_t smem);

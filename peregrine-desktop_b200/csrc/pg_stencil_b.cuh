@@ -68,6 +68,18 @@ template <> struct BUnpack<__nv_bfloat16> {
     }
 };
 
+template <> struct BUnpack<Q16> {
+    static __device__ __forceinline__ void fma(const uint4 q, float w, float (&a)[8]) {
+        const uint32_t v[4] = {q.x, q.y, q.z, q.w};
+        const float ws = w * kQ16Step;  // an exact power-of-two scaling
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            a[2 * k] = fmaf(ws, (float)(v[k] & 0xffffu), a[2 * k]);
+            a[2 * k + 1] = fmaf(ws, (float)(v[k] >> 16), a[2 * k + 1]);
+        }
+    }
+};
+
 // Shared memory of one block: two record slots, the control order, two
 // window buffers and two sets of per-row / per-column successor corners.
 __host__ __device__ inline size_t stencil_b_smem(int nctl, int tile_x, int n2) {
@@ -346,8 +358,8 @@ __global__ void __launch_bounds__(256)
 // flag is set only clear their residual slot.  The two value buffers of a
 // table alternate with `parity`.
 
-template <typename S>
-__global__ void __launch_bounds__(256)
+template <typename S, bool VEC>
+__global__ void __launch_bounds__(256, 4)
     k_stencil_b_batch(const BatchTable* __restrict__ tabs, int ntab, int64_t nitems, int parity,
                       const int32_t* __restrict__ done, double* part_sum, double* part_max) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -360,18 +372,16 @@ __global__ void __launch_bounds__(256)
         }
         const BatchTable& tb = tabs[lo];
         __syncthreads();  // the previous item's shared memory is free
-        if (done[lo]) {
-            if (threadIdx.x == 0) { part_sum[it] = 0.0; part_max[it] = 0.0; }
+        // tables of the other vector class and converged tables only clear
+        // their slot (the other class has its own launch)
+        if (done[lo] || (tb.vec != 0) != VEC) {
+            if (threadIdx.x == 0 && done[lo]) { part_sum[it] = 0.0; part_max[it] = 0.0; }
             continue;
         }
         const S* vin = static_cast<const S*>(tb.V[parity]);
         S* vout = const_cast<S*>(static_cast<const S*>(tb.V[1 - parity]));
-        if (tb.vec)
-            stencil_b_item<S, false, true>(vin, vout, tb.occ, tb.mask, tb.recs, tb.kp, tb.order,
-                                           part_sum, part_max, nullptr, it - tb.item0, it, smem_raw);
-        else
-            stencil_b_item<S, false, false>(vin, vout, tb.occ, tb.mask, tb.recs, tb.kp, tb.order,
-                                            part_sum, part_max, nullptr, it - tb.item0, it, smem_raw);
+        stencil_b_item<S, false, VEC>(vin, vout, tb.occ, tb.mask, tb.recs, tb.kp, tb.order,
+                                      part_sum, part_max, nullptr, it - tb.item0, it, smem_raw);
     }
 }
 

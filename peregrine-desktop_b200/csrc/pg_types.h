@@ -20,6 +20,13 @@ constexpr int kBMaxTileCells = 1024;
 // Model entries the adjoint differentiates (diagonals of B, A, S, D; q; c).
 constexpr int kNThetaHost = 18;
 
+// Q16 storage: V = u * kQ16Step seconds, u an unsigned 16-bit code.
+struct Q16 {
+    uint16_t u;
+};
+constexpr float kQ16Step = 1.0f / 2048.0f;
+constexpr float kQ16Scale = 2048.0f;
+
 // Everything a sweep kernel needs besides the arrays, passed by value.
 struct KParams {
     pg_grid6 g;

@@ -17,34 +17,39 @@ from .synth import Problem
 
 
 def tile_candidates(n1: int, n2: int) -> list[int]:
-    """Rows per block worth trying: whole rows, at most 1024 cells per block,
-    each count of tiles per plane once."""
+    """Rows per block worth trying in a batch (256-thread blocks, 4 cells per
+    thread): whole rows, at most 1024 cells per block and at least 3/4 of the
+    largest tile, each count of tiles per plane once."""
     rmax = min(n1, 1024 // n2)
+    floor_cells = 0.75 * rmax * n2
     out = []
     for nt in range(-(-n1 // rmax), n1 + 1):
         r = -(-n1 // nt)
-        if r < 2 or len(out) >= 4:
+        if r * n2 < floor_cells or len(out) >= 4:
             break
         if r not in out:
             out.append(r)
     return out or [rmax]
 
 
-def autotune(problems, device: int = 0, steps: int = 3) -> dict:
-    """{(n1, n2): rows} for the problems' position shapes, each the fastest
-    candidate in device-timed sweeps of one table of that shape."""
+def autotune(problems, device: int = 0, sweeps: int = 4) -> dict:
+    """{(n1, n2): rows} for the problems' position shapes: each candidate
+    tiling timed as a one-table batch (the launch the batch runs) on one
+    table of that shape, the fastest kept."""
     best = {}
     for pr in problems:
         n1, n2 = int(pr.grid.n[0]), int(pr.grid.n[1])
         if (n1, n2) in best:
             continue
-        with _lib.Context(device) as ctx:
-            ctx.load_problem(pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.ctl, "fp16")
-            ctx.solve(pr.seeds, 0, 0.0, _lib.default_opts(kernel=_lib.KERNEL_STENCIL, storage="fp16"))
-            times = {}
-            for r in tile_candidates(n1, n2):
-                ctx.set_tile_rows(r)
-                times[r] = ctx.time_sweeps(1, steps, _lib.KERNEL_STENCIL)
+        cands = tile_candidates(n1, n2)
+        if len(cands) == 1:
+            best[(n1, n2)] = cands[0]
+            continue
+        times = {}
+        for r in cands:
+            with _lib.Batch(device, "fp16") as b:
+                b.add(pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.seeds, pr.ctl, r)
+                times[r] = b.solve(sweeps, 0.0, 0, True).kernel_ms
         best[(n1, n2)] = min(times, key=times.get)
     return best
 

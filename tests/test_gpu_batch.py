@@ -44,7 +44,7 @@ def test_batch_16bit_with_polish_matches_fp32(problems, storage):
 
 
 def test_autotune_picks_a_candidate(problems):
-    tiles = pb.autotune(problems[:2], steps=2)
+    tiles = pb.autotune(problems[:2], sweeps=2)
     for (n1, n2), r in tiles.items():
         assert r in pb.tile_candidates(n1, n2)
     res, _, _ = pb.solve_batch(problems, storage="fp16", iters=3000, tol=1e-4, tiles=tiles)

@@ -92,7 +92,7 @@ def test_one_sweep_fma_stencil_within_tolerance(og, tiny, tiny_state, kernel):
     assert np.mean(gam[free] == am[free]) >= ARGMIN_AGREE
 
 
-@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16", "q16"])
 @pytest.mark.parametrize("n", [(40, 48, 8, 5, 5, 5), (36, 44, 8, 5, 5, 5)])
 def test_one_sweep_blend_tiles(og, n, storage):
     """The blend-then-shift sweep on grids that need several row tiles per
@@ -112,6 +112,8 @@ def test_one_sweep_blend_tiles(og, n, storage):
         got = ctx.get_value()
     if storage == "fp32":
         half_ulp = 0.0
+    elif storage == "q16":
+        half_ulp = 2.0 ** -12
     else:
         mant = 10 if storage == "fp16" else 7
         half_ulp = np.ldexp(1.0, np.frexp(np.abs(want).astype(np.float64))[1] - 1 - mant - 1)
