@@ -101,7 +101,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    p = Path(path or os.environ.get("PEREGRINE_HJB_LIB") or LIB_PATH)
     if not p.exists():
         raise RuntimeError(
             f"{p} is missing: build the CUDA library first "

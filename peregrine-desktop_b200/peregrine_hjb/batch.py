@@ -18,18 +18,18 @@ from .synth import Problem
 
 def tile_candidates(n1: int, n2: int) -> list[int]:
     """Rows per block worth trying in a batch (256-thread blocks, 4 cells per
-    thread): whole rows, at most 1024 cells per block and at least 3/4 of the
-    largest tile, each count of tiles per plane once."""
+    thread): whole rows, tiles of equal height, at most 1024 cells per block
+    and at least 3/4 of the balanced tiling with the fewest tiles."""
     rmax = min(n1, 1024 // n2)
-    floor_cells = 0.75 * rmax * n2
+    r0 = -(-n1 // -(-n1 // rmax))  # the balanced tiling with the fewest tiles
     out = []
     for nt in range(-(-n1 // rmax), n1 + 1):
         r = -(-n1 // nt)
-        if r * n2 < floor_cells or len(out) >= 4:
+        if r * n2 < 0.75 * r0 * n2 or len(out) >= 4:
             break
         if r not in out:
             out.append(r)
-    return out or [rmax]
+    return out
 
 
 def autotune(problems, device: int = 0, sweeps: int = 4) -> dict:
