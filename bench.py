@@ -373,9 +373,7 @@ def run_accuracy(args, local_rank):
     base = (pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.seeds, pr.ctl)
 
     def solve(storage, tol, polish=0):
-        kw = dict(storage=storage)
-        if polish:
-            kw["polish_sweeps"] = polish
+        kw = dict(storage=storage, polish_sweeps=polish)
         opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL, **kw)
         return _lib.solve_value(*base, 20000 if tol < 1e-8 else args.max_sweeps, tol, opts,
                                 device=local_rank)
@@ -390,8 +388,10 @@ def run_accuracy(args, local_rank):
     runs, ttc = {}, {}
     for name in args.storages.split(","):
         runs[name] = []
+        store = name.replace("-nopolish", "")
+        polish = 0 if (store == "fp32" or name.endswith("-nopolish")) else args.max_sweeps
         for tol in (1e-4, 3e-5, 1e-5, 3e-6):
-            V, res = solve(name, tol, 0 if name == "fp32" else args.max_sweeps)
+            V, res = solve(store, tol, polish)
             V = V.astype(np.float64)
             err = np.abs(V - ref32)[reached]
             e64 = np.abs(V - ref64)[reached]
@@ -433,7 +433,8 @@ def main():
     ap.add_argument("--accuracy", action="store_true",
                     help="time-to-converge and FP32/FP64/FP16/BF16 error report instead of "
                          "the throughput line")
-    ap.add_argument("--storages", default="fp32,fp16,bf16,q16")
+    ap.add_argument("--storages", default="fp32,fp16,bf16,q16,q16-nopolish",
+                    help="storages of the accuracy report; -nopolish: no FP32 polish")
     ap.add_argument("--storage", default="fp32",
                     help="storage of V for --only-device timing (the benchmark line is FP32)")
     ap.add_argument("--max-sweeps", type=int, default=4000)

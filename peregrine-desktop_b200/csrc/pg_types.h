@@ -74,6 +74,7 @@ struct BatchTable {
     int32_t pad;
     KParams kp;
 };
+static_assert(sizeof(BatchTable) % 4 == 0, "BatchTable is copied as 32-bit words");
 
 // Records msg as the text pg_last_error returns on this thread; returns code.
 int set_last_error(int code, const std::string& msg);
