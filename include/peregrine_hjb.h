@@ -223,8 +223,10 @@ int pg_launch_count(pg_ctx* ctx, int64_t* launches);
 int pg_set_tile_rows(pg_ctx* ctx, int32_t rows);
 
 /* ------------------------------------------------------------------ */
-/* batched solves: many independent tables, one persistent launch per  */
-/* sweep over all of them, captured in a CUDA graph.  The reference     */
+/* batched solves: many independent tables swept side by side: per     */
+/* sweep one persistent launch for each block size among the tables    */
+/* (one launch when they share it), captured in a CUDA graph.  The     */
+/* reference                                                            */
 /* solves its targets one after another (Run.jl:1851-1958); this is the */
 /* same per-table solve_value!, run side by side.                       */
 /* ------------------------------------------------------------------ */

@@ -985,14 +985,30 @@ struct pg_batch {
 namespace {
 
 // Descriptors of every table at storage `st` (the V buffers of each
-// context, its masks and records); smem_out = the largest shared memory.
-int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, int64_t* nitems,
-                      size_t* smem_out) {
+// context, its masks and records), ordered by the tables' block size so each
+// block size is one contiguous item range; perm[k] = the table of
+// descriptor k; smem_out = the largest shared memory.
+struct BatchGroup {
+    int64_t first, count;
+    int threads;
+    bool any_vec, any_scalar;
+};
+
+int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, std::vector<int>& perm,
+                      std::vector<BatchGroup>& groups, int64_t* nitems, size_t* smem_out) {
     d.clear();
+    groups.clear();
+    const int ntab = (int)b->tabs.size();
+    perm.resize(ntab);
+    for (int t = 0; t < ntab; ++t) perm[t] = t;
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int c) {
+        return b->tabs[a]->kp.bblock < b->tabs[c]->kp.bblock;
+    });
     int64_t item = 0;
     size_t smem = 0;
     const int vn = 16 / (int)elem_bytes(st);
-    for (pg_ctx* c : b->tabs) {
+    for (int k = 0; k < ntab; ++k) {
+        pg_ctx* c = b->tabs[perm[k]];
         pg::BatchTable t{};
         t.V[0] = c->V[0];
         t.V[1] = c->V[1];
@@ -1006,6 +1022,10 @@ int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, int64
         t.item0 = item;
         t.nitems = c->kp.nplanes * c->kp.btiles_x;
         t.vec = c->kp.g.n[1] % vn == 0 ? 1 : 0;
+        if (groups.empty() || groups.back().threads != c->kp.bblock)
+            groups.push_back(BatchGroup{item, 0, c->kp.bblock, false, false});
+        groups.back().count += t.nitems;
+        (t.vec ? groups.back().any_vec : groups.back().any_scalar) = true;
         item += t.nitems;
         smem = std::max(smem, pg::stencil_b_smem_bytes(c->kp));
         d.push_back(t);
@@ -1020,9 +1040,11 @@ int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, int64
 int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_graph,
                 double* kms, int32_t* steps_sweeps) {
     std::vector<pg::BatchTable> d;
+    std::vector<int> perm;
+    std::vector<BatchGroup> groups;
     int64_t nitems = 0;
     size_t smem = 0;
-    batch_descriptors(b, st, d, &nitems, &smem);
+    batch_descriptors(b, st, d, perm, groups, &nitems, &smem);
     const int ntab = (int)b->tabs.size();
     if (nitems > b->cap_items || ntab > b->cap_tabs) {
         b->free_bufs();
@@ -1038,23 +1060,26 @@ int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_gr
     }
     PG_CUDA(cudaMemcpyAsync(b->tabs_d, d.data(), sizeof(pg::BatchTable) * ntab,
                             cudaMemcpyHostToDevice, b->stream));
-    for (int t = 0; t < ntab; ++t) b->done_h[t] = 0;
+    for (int k = 0; k < ntab; ++k) b->done_h[k] = 0;
     PG_CUDA(cudaMemcpyAsync(b->done_d, b->done_h, sizeof(int32_t) * ntab, cudaMemcpyHostToDevice,
                             b->stream));
     int sms = 0;
     PG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    const int per_sm = pg::batch_blocks_per_sm(st, smem);
-    if (per_sm <= 0) return fail(PG_EUNSUPPORTED, "the batched sweep does not fit on an SM");
-    const int grid = (int)std::min<int64_t>(nitems, (int64_t)sms * per_sm);
-    bool any_vec = false, any_scalar = false;
-    for (const auto& t : d) (t.vec ? any_vec : any_scalar) = true;
+    std::vector<int> grids;
+    for (const BatchGroup& gr : groups) {
+        const int per_sm = pg::batch_blocks_per_sm(st, smem, gr.threads);
+        if (per_sm <= 0) return fail(PG_EUNSUPPORTED, "the batched sweep does not fit on an SM");
+        grids.push_back((int)std::min<int64_t>(gr.count, (int64_t)sms * per_sm));
+    }
 
     auto step = [&](cudaStream_t s) -> cudaError_t {
         cudaError_t e = cudaSuccess;
         for (int parity = 0; parity < 2 && e == cudaSuccess; ++parity) {
-            e = pg::launch_stencil_b_batch(st, b->tabs_d, ntab, nitems, parity, b->done_d,
-                                           b->part_sum, b->part_max, smem, grid, any_vec,
-                                           any_scalar, s);
+            for (size_t g = 0; g < groups.size() && e == cudaSuccess; ++g)
+                e = pg::launch_stencil_b_batch(st, b->tabs_d, ntab, groups[g].first,
+                                               groups[g].count, groups[g].threads, parity,
+                                               b->done_d, b->part_sum, b->part_max, smem, grids[g],
+                                               groups[g].any_vec, groups[g].any_scalar, s);
             if (e == cudaSuccess)
                 e = pg::launch_reduce_batch(b->tabs_d, ntab, b->part_sum, b->part_max, b->out_d, s);
         }
@@ -1095,11 +1120,12 @@ int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_gr
         *kms += ms;
         done_sw += 2;
         int left = 0;
-        for (int t = 0; t < ntab; ++t) {
-            if (b->done_h[t]) continue;
+        for (int k = 0; k < ntab; ++k) {
+            if (b->done_h[k]) continue;
+            const int t = perm[k];
             b->sweeps[t] += 2;
-            b->last_max[t] = b->out_h[2 * t + 1];
-            if (b->last_max[t] <= tol) b->done_h[t] = 1;
+            b->last_max[t] = b->out_h[2 * k + 1];
+            if (b->last_max[t] <= tol) b->done_h[k] = 1;
             else ++left;
         }
         if (!left) break;

@@ -947,10 +947,10 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t nitems,
-                                   int parity, const int32_t* done, double* part_sum,
-                                   double* part_max, size_t smem, int grid, bool any_vec,
-                                   bool any_scalar, cudaStream_t st) {
+cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
+                                   int64_t count, int threads, int parity, const int32_t* done,
+                                   double* part_sum, double* part_max, size_t smem, int grid,
+                                   bool any_vec, bool any_scalar, cudaStream_t st) {
 #define PG_BB(S)                                                                                 \
     {                                                                                            \
         static bool attr_set = false;                                                            \
@@ -965,14 +965,17 @@ cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab
             attr_set = true;                                                                     \
         }                                                                                        \
         if (any_vec)                                                                             \
-            k_stencil_b_batch<S, true><<<grid, 256, smem, st>>>(tabs, ntab, nitems, parity, done, \
-                                                                part_sum, part_max);             \
+            k_stencil_b_batch<S, true><<<grid, threads, smem, st>>>(tabs, ntab, first, count,    \
+                                                                    parity, done, part_sum,      \
+                                                                    part_max);                   \
         if (any_scalar)                                                                          \
-            k_stencil_b_batch<S, false><<<grid, 256, smem, st>>>(tabs, ntab, nitems, parity,     \
-                                                                 done, part_sum, part_max);      \
+            k_stencil_b_batch<S, false><<<grid, threads, smem, st>>>(tabs, ntab, first, count,   \
+                                                                     parity, done, part_sum,     \
+                                                                     part_max);                  \
         return cudaGetLastError();                                                               \
     }
-    if (smem > 200 * 1024 || grid <= 0) return cudaErrorInvalidValue;
+    if (smem > 200 * 1024 || grid <= 0 || threads <= 0 || threads > 256 || threads % 32)
+        return cudaErrorInvalidValue;
     switch (storage) {
         case PG_STORE_F32: PG_BB(float)
         case PG_STORE_F16: PG_BB(__half)
@@ -989,28 +992,25 @@ cudaError_t launch_reduce_batch(const BatchTable* tabs, int ntab, const double* 
     return cudaGetLastError();
 }
 
-int batch_blocks_per_sm(int storage, size_t smem) {
+template <typename S>
+static int batch_occupancy(int threads, size_t smem) {
     int nb = 0;
-    cudaError_t e = cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_stencil_b_batch<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<S, true>, threads,
+                                                      smem) != cudaSuccess)
+        return 0;
+    return nb;
+}
+
+int batch_blocks_per_sm(int storage, size_t smem, int threads) {
     switch (storage) {
-        case PG_STORE_F32:
-            cudaFuncSetAttribute(k_stencil_b_batch<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<float, true>, 256, smem);
-            break;
-        case PG_STORE_F16:
-            cudaFuncSetAttribute(k_stencil_b_batch<__half, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__half, true>, 256, smem);
-            break;
-        case PG_STORE_BF16:
-            cudaFuncSetAttribute(k_stencil_b_batch<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<__nv_bfloat16, true>, 256, smem);
-            break;
-        case PG_STORE_Q16:
-            cudaFuncSetAttribute(k_stencil_b_batch<Q16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<Q16, true>, 256, smem);
-            break;
+        case PG_STORE_F32: return batch_occupancy<float>(threads, smem);
+        case PG_STORE_F16: return batch_occupancy<__half>(threads, smem);
+        case PG_STORE_BF16: return batch_occupancy<__nv_bfloat16>(threads, smem);
+        case PG_STORE_Q16: return batch_occupancy<Q16>(threads, smem);
     }
-    return e == cudaSuccess ? nb : 0;
+    return 0;
 }
 
 size_t stencil_b_smem_bytes(const KParams& kp) {

@@ -45,13 +45,13 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
                              const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                              cudaStream_t st, int64_t* launches);
 size_t stencil_b_smem_bytes(const KParams& kp);
-cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t nitems,
-                                   int parity, const int32_t* done, double* part_sum,
-                                   double* part_max, size_t smem, int grid, bool any_vec,
-                                   bool any_scalar, cudaStream_t st);
+cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
+                                   int64_t count, int threads, int parity, const int32_t* done,
+                                   double* part_sum, double* part_max, size_t smem, int grid,
+                                   bool any_vec, bool any_scalar, cudaStream_t st);
 cudaError_t launch_reduce_batch(const BatchTable* tabs, int ntab, const double* part_sum,
                                 const double* part_max, double* out, cudaStream_t st);
-int batch_blocks_per_sm(int storage, size_t smem);
+int batch_blocks_per_sm(int storage, size_t smem, int threads);
 cudaError_t launch_adj_active(const float* V, const int16_t* pol, const uint8_t* occ,
                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                               uint8_t* active, cudaStream_t st);

@@ -355,21 +355,23 @@ __global__ void __launch_bounds__(256, 5)
 
 // Many tables in one launch (BatchTable, pg_types.h).  Work items of all
 // tables are numbered contiguously (table t owns items [item0, item0 +
-// nitems)); a persistent grid walks them, and items of a table whose `done`
-// flag is set only clear their residual slot.  The two value buffers of a
-// table alternate with `parity`.
+// nitems)); a persistent grid walks the items [first, first + count) -- the
+// tables sharing one block size -- and items of a table whose `done` flag is
+// set only clear their residual slot.  The two value buffers of a table
+// alternate with `parity`.
 
 template <typename S, bool VEC>
 __global__ void __launch_bounds__(256, 4)
-    k_stencil_b_batch(const BatchTable* __restrict__ tabs, int ntab, int64_t nitems, int parity,
-                      const int32_t* __restrict__ done, double* part_sum, double* part_max) {
+    k_stencil_b_batch(const BatchTable* __restrict__ tabs, int ntab, int64_t first, int64_t count,
+                      int parity, const int32_t* __restrict__ done, double* part_sum,
+                      double* part_max) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // the current table's descriptor, in shared memory so that its many
     // fields are read from there rather than held in registers
     __shared__ __align__(16) BatchTable tb;
     __shared__ int cur;
     if (threadIdx.x == 0) cur = -1;
-    for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+    for (int64_t it = first + blockIdx.x; it < first + count; it += gridDim.x) {
         int lo = 0, hi = ntab - 1;  // the table owning item `it`
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
