@@ -992,6 +992,7 @@ struct BatchGroup {
     int64_t first, count;
     int threads;
     bool any_vec, any_scalar;
+    bool off32;  // every table of the group has fewer than 2^32 cells
 };
 
 int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, std::vector<int>& perm,
@@ -1023,8 +1024,9 @@ int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, std::
         t.nitems = c->kp.nplanes * c->kp.btiles_x;
         t.vec = c->kp.g.n[1] % vn == 0 ? 1 : 0;
         if (groups.empty() || groups.back().threads != c->kp.bblock)
-            groups.push_back(BatchGroup{item, 0, c->kp.bblock, false, false});
+            groups.push_back(BatchGroup{item, 0, c->kp.bblock, false, false, true});
         groups.back().count += t.nitems;
+        if (c->kp.ncells > (int64_t)0xffffffffLL) groups.back().off32 = false;
         (t.vec ? groups.back().any_vec : groups.back().any_scalar) = true;
         item += t.nitems;
         smem = std::max(smem, pg::stencil_b_smem_bytes(c->kp));
@@ -1079,7 +1081,8 @@ int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_gr
                 e = pg::launch_stencil_b_batch(st, b->tabs_d, ntab, groups[g].first,
                                                groups[g].count, groups[g].threads, parity,
                                                b->done_d, b->part_sum, b->part_max, smem, grids[g],
-                                               groups[g].any_vec, groups[g].any_scalar, s);
+                                               groups[g].any_vec, groups[g].any_scalar,
+                                               groups[g].off32, s);
             if (e == cudaSuccess)
                 e = pg::launch_reduce_batch(b->tabs_d, ntab, b->part_sum, b->part_max, b->out_d, s);
         }

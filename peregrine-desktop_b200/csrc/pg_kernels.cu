@@ -885,19 +885,19 @@ cudaError_t launch_stencil_u(int storage, const void* Vin, void* Vout, const uin
     return cudaErrorInvalidValue;
 }
 
-template <typename S, bool ARGMIN, bool VEC>
+template <typename S, bool ARGMIN, bool VEC, bool OFF32>
 static cudaError_t stencil_b_v(const void* Vin, void* Vout, const uint8_t* occ,
                                const uint32_t* mask, const uint32_t* recs, const KParams& kb,
                                const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                                int64_t blocks, int threads, size_t smem, cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_stencil_b<S, ARGMIN, VEC>,
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_b<S, ARGMIN, VEC, OFF32>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    k_stencil_b<S, ARGMIN, VEC><<<(unsigned)blocks, threads, smem, st>>>(
+    k_stencil_b<S, ARGMIN, VEC, OFF32><<<(unsigned)blocks, threads, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, mask, recs, kb, order, sb.part_sum, sb.part_max, argmin);
     return cudaSuccess;
 }
@@ -918,10 +918,12 @@ static cudaError_t stencil_b_t(const void* Vin, void* Vout, const uint8_t* occ,
     const size_t smem = stencil_b_smem(kp.nctl, kp.btile_x, kp.g.n[1]);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     const bool vec = kp.g.n[1] % BVec<S>::N == 0;
-    cudaError_t e = vec ? stencil_b_v<S, ARGMIN, true>(Vin, Vout, occ, mask, recs, kb, order, sb,
-                                                        argmin, blocks, kp.bblock, smem, st)
-                        : stencil_b_v<S, ARGMIN, false>(Vin, Vout, occ, mask, recs, kb, order, sb,
-                                                         argmin, blocks, kp.bblock, smem, st);
+    const bool off32 = kp.ncells <= (int64_t)0xffffffffLL;
+#define PG_SBV(V, O) stencil_b_v<S, ARGMIN, V, O>(Vin, Vout, occ, mask, recs, kb, order, sb, argmin, \
+                                                  blocks, kp.bblock, smem, st)
+    cudaError_t e = vec ? (off32 ? PG_SBV(true, true) : PG_SBV(true, false))
+                        : (off32 ? PG_SBV(false, true) : PG_SBV(false, false));
+#undef PG_SBV
     if (e != cudaSuccess) return e;
     k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
     *launches += 2;
@@ -950,28 +952,39 @@ cudaError_t launch_stencil_b(int storage, const void* Vin, void* Vout, const uin
 cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
                                    int64_t count, int threads, int parity, const int32_t* done,
                                    double* part_sum, double* part_max, size_t smem, int grid,
-                                   bool any_vec, bool any_scalar, cudaStream_t st) {
+                                   bool any_vec, bool any_scalar, bool off32, cudaStream_t st) {
 #define PG_BB(S)                                                                                 \
     {                                                                                            \
         static bool attr_set = false;                                                            \
         if (!attr_set) {                                                                         \
-            cudaError_t e = cudaFuncSetAttribute(k_stencil_b_batch<S, true>,                     \
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                                 200 * 1024);                                    \
-            if (e == cudaSuccess)                                                                \
-                e = cudaFuncSetAttribute(k_stencil_b_batch<S, false>,                            \
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); \
+            cudaError_t e = cudaSuccess;                                                         \
+            void (*fns[4])(const BatchTable*, int, int64_t, int64_t, int, const int32_t*,        \
+                           double*, double*) = {k_stencil_b_batch<S, true, true>,                \
+                                                k_stencil_b_batch<S, true, false>,               \
+                                                k_stencil_b_batch<S, false, true>,               \
+                                                k_stencil_b_batch<S, false, false>};             \
+            for (int f = 0; f < 4 && e == cudaSuccess; ++f)                                      \
+                e = cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                         200 * 1024);                                            \
             if (e != cudaSuccess) return e;                                                      \
             attr_set = true;                                                                     \
         }                                                                                        \
-        if (any_vec)                                                                             \
-            k_stencil_b_batch<S, true><<<grid, threads, smem, st>>>(tabs, ntab, first, count,    \
-                                                                    parity, done, part_sum,      \
-                                                                    part_max);                   \
-        if (any_scalar)                                                                          \
-            k_stencil_b_batch<S, false><<<grid, threads, smem, st>>>(tabs, ntab, first, count,   \
-                                                                     parity, done, part_sum,     \
-                                                                     part_max);                  \
+        if (any_vec) {                                                                           \
+            if (off32)                                                                           \
+                k_stencil_b_batch<S, true, true><<<grid, threads, smem, st>>>(                   \
+                    tabs, ntab, first, count, parity, done, part_sum, part_max);                 \
+            else                                                                                 \
+                k_stencil_b_batch<S, true, false><<<grid, threads, smem, st>>>(                  \
+                    tabs, ntab, first, count, parity, done, part_sum, part_max);                 \
+        }                                                                                        \
+        if (any_scalar) {                                                                        \
+            if (off32)                                                                           \
+                k_stencil_b_batch<S, false, true><<<grid, threads, smem, st>>>(                  \
+                    tabs, ntab, first, count, parity, done, part_sum, part_max);                 \
+            else                                                                                 \
+                k_stencil_b_batch<S, false, false><<<grid, threads, smem, st>>>(                 \
+                    tabs, ntab, first, count, parity, done, part_sum, part_max);                 \
+        }                                                                                        \
         return cudaGetLastError();                                                               \
     }
     if (smem > 200 * 1024 || grid <= 0 || threads <= 0 || threads > 256 || threads % 32)
@@ -995,10 +1008,10 @@ cudaError_t launch_reduce_batch(const BatchTable* tabs, int ntab, const double* 
 template <typename S>
 static int batch_occupancy(int threads, size_t smem) {
     int nb = 0;
-    cudaFuncSetAttribute(k_stencil_b_batch<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_stencil_b_batch<S, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          200 * 1024);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<S, true>, threads,
-                                                      smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_b_batch<S, true, false>,
+                                                      threads, smem) != cudaSuccess)
         return 0;
     return nb;
 }

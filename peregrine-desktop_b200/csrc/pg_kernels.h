@@ -48,7 +48,7 @@ size_t stencil_b_smem_bytes(const KParams& kp);
 cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
                                    int64_t count, int threads, int parity, const int32_t* done,
                                    double* part_sum, double* part_max, size_t smem, int grid,
-                                   bool any_vec, bool any_scalar, cudaStream_t st);
+                                   bool any_vec, bool any_scalar, bool off32, cudaStream_t st);
 cudaError_t launch_reduce_batch(const BatchTable* tabs, int ntab, const double* part_sum,
                                 const double* part_max, double* out, cudaStream_t st);
 int batch_blocks_per_sm(int storage, size_t smem, int threads);
