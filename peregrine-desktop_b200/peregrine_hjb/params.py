@@ -9,7 +9,8 @@ Additive job-JSON keys (absent = the reference's behaviour):
                 "cube3" = {-1,0,1}^3, "cube5" = {-1,-0.5,0,0.5,1}^3
   target_region {"kind": "disk", "radius_cm": r, "speed_max_cm_s": s}
   stop_rule     "l1_quiet" (default) | "maxnorm"
-  storage       "fp32" (default) | "fp16" | "bf16" | "fp64"
+  storage       "fp32" (default) | "fp16" | "bf16" | "q16" (16-bit fixed point,
+                2^-11 s steps, value_cap below 32 s) | "fp64"
   polish_sweeps FP32 sweeps allowed after a 16-bit solve converges (64)
   sweep         "jacobi" (the only sweep order on the GPU)
 """

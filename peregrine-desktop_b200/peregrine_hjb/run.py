@@ -366,7 +366,7 @@ def plan(cfg) -> dict:
     reads, computed from the same grid construction as the solve."""
     prep = Prepared(cfg)
     g, sp = prep.g, prep.sp
-    elem = {"fp32": 4, "fp16": 2, "bf16": 2, "fp64": 8}[sp.storage]
+    elem = {"fp32": 4, "fp16": 2, "bf16": 2, "q16": 2, "fp64": 8}[sp.storage]
     need = 2 * prep.cells * elem + (3 * prep.cells if sp.warm else 0)
     return {
         "cells": prep.cells,
