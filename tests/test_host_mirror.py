@@ -110,6 +110,15 @@ def test_solver_params_defaults():
     assert sp.nctl == 67 and sp.warm and sp.iters == 400 and sp.tol == 1e-3
 
 
+def test_storage_key_accepts_the_library_storages():
+    g = pgrid.Grid6.make((4, 4, 4, 3, 3, 3), (0, 0, 0, -1, -1, -1), (1, 1, 1, 1, 1, 1))
+    for name in ("fp32", "fp16", "bf16", "q16", "fp64"):
+        assert pparams.solver_params({"storage": name}, g).storage == name
+    import pytest
+    with pytest.raises(ValueError):
+        pparams.solver_params({"storage": "fp8"}, g)
+
+
 def test_region_seeds_are_disk_and_slow():
     from peregrine_hjb.synth import Problem
     pr = Problem("small", seed=1)
