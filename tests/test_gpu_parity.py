@@ -334,3 +334,13 @@ def test_full_size_properties():
     assert float(np.max(diff)) == dm
     assert abs(float(np.sum(diff)) - d) <= 1e-9 * max(1.0, d)
     assert np.count_nonzero(V2 < cap) > np.count_nonzero(V1 < cap) or dm == 0
+
+
+def test_measured_peaks_are_plausible():
+    """The on-chip probes behind the secondary rooflines: positive and below
+    generous bounds for any current GPU (shared memory < 1e6 GB/s, L2 < 1e5
+    GB/s, FP32 FMA < 1e3 TFLOP/s)."""
+    pk = _lib.measure_peaks(0)
+    assert 0 < pk["smem_gbs"] < 1e6
+    assert 0 < pk["l2_gbs"] < 1e5
+    assert 0 < pk["fma_tflops"] < 1e3
