@@ -33,7 +33,7 @@ def test_batch_matches_individual_solves(problems, graph):
         assert np.array_equal(V, want), f"max |dV| {np.max(np.abs(V - want))}"
 
 
-@pytest.mark.parametrize("storage", ["fp16", "bf16"])
+@pytest.mark.parametrize("storage", ["fp16", "bf16", "q16"])
 def test_batch_16bit_with_polish_matches_fp32(problems, storage):
     _, V32, _ = pb.solve_batch(problems, storage="fp32", iters=3000, tol=1e-5)
     res, V16, info = pb.solve_batch(problems, storage=storage, iters=3000, tol=1e-5,
