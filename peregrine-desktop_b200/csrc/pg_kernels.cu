@@ -647,6 +647,14 @@ __global__ void k_encode(const S* V, KParams kp, int32_t dtype, double scale, do
 // ---------------------------------------------------------------------------
 // host-side launchers
 // ---------------------------------------------------------------------------
+// Kernel attributes (the dynamic shared-memory ceiling) are per device; each
+// launch site sets them once per device it runs on.
+static inline uint64_t device_bit() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d >= 0 && d < 64 ? (1ull << d) : 0ull;
+}
+
 static inline int grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     if (b > (int64_t)148 * 64) b = (int64_t)148 * 64;
@@ -775,12 +783,13 @@ static cudaError_t stencil_t(const void* Vin, void* Vout, const uint8_t* occ, co
     const int64_t blocks = stencil_blocks(kp);
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const size_t smem = stencil_smem_bytes<T, EXACT>(kp.nctl, kp.nsub, kp.nchk);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil<S, T, EXACT, NSUB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set |= attr_bit;
     }
     k_stencil<S, T, EXACT, NSUB><<<(unsigned)blocks, kp.block, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, kp, ctl, order, sb.part_sum, sb.part_max, argmin);
@@ -823,12 +832,13 @@ cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const flo
     const int coltab = kp.g.n[1] <= 255 && kp.nchk <= 4 && smem + tab <= 200 * 1024;
     if (coltab) smem += tab;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_prep,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set |= attr_bit;
     }
     if (kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
     k_stencil_prep<<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask, recs, coltab);
@@ -853,12 +863,13 @@ static cudaError_t stencil_u_t(const void* Vin, void* Vout, const uint8_t* occ,
     const int64_t blocks = kp.nplanes * kp.utiles_x;
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const size_t smem = stencil_u_smem(kp.nctl);
-    static bool attr_set = false;
-    if (!attr_set) {
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_u<S, kURX, R, ARGMIN>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set |= attr_bit;
     }
     k_stencil_u<S, kURX, R, ARGMIN><<<(unsigned)blocks, kp.ublock, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, mask, recs, ku, order, sb.part_sum, sb.part_max, argmin);
@@ -890,12 +901,13 @@ static cudaError_t stencil_b_v(const void* Vin, void* Vout, const uint8_t* occ,
                                const uint32_t* mask, const uint32_t* recs, const KParams& kb,
                                const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                                int64_t blocks, int threads, size_t smem, cudaStream_t st) {
-    static bool attr_set = false;
-    if (!attr_set) {
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_b<S, ARGMIN, VEC, OFF32>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set |= attr_bit;
     }
     k_stencil_b<S, ARGMIN, VEC, OFF32><<<(unsigned)blocks, threads, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, mask, recs, kb, order, sb.part_sum, sb.part_max, argmin);
@@ -955,8 +967,9 @@ cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab
                                    bool any_vec, bool any_scalar, bool off32, cudaStream_t st) {
 #define PG_BB(S)                                                                                 \
     {                                                                                            \
-        static bool attr_set = false;                                                            \
-        if (!attr_set) {                                                                         \
+        static uint64_t attr_set = 0;                                                            \
+        const uint64_t attr_bit = device_bit();                                                  \
+        if (!(attr_set & attr_bit)) {                                                                         \
             cudaError_t e = cudaSuccess;                                                         \
             void (*fns[4])(const BatchTable*, int, int64_t, int64_t, int, const int32_t*,        \
                            double*, double*) = {k_stencil_b_batch<S, true, true>,                \
@@ -967,7 +980,7 @@ cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab
                 e = cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                          200 * 1024);                                            \
             if (e != cudaSuccess) return e;                                                      \
-            attr_set = true;                                                                     \
+            attr_set |= attr_bit;                                                                     \
         }                                                                                        \
         if (any_vec) {                                                                           \
             if (off32)                                                                           \
@@ -1065,12 +1078,13 @@ cudaError_t launch_adj_grad(const float* V, const float* lam, const int16_t* pol
                             const float* ctl, double* grad, cudaStream_t st) {
     const size_t smem = adj_grad_smem(kp.nctl);
     if (smem > 200 * 1024 || kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_adj_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set |= attr_bit;
     }
     k_adj_grad<<<(unsigned)kp.nplanes, 128, smem, st>>>(V, lam, pol, active, recs, kp, ctl, grad);
     return cudaGetLastError();
