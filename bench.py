@@ -80,6 +80,20 @@ def onchip_rooflines(pr, rate_per_gpu: float, elem: int, peaks_onchip) -> dict:
     return out
 
 
+def profiled_value(key: str):
+    """A number from the committed ncu summary of the sweep kernel (a line
+    `key: N ...`), or None."""
+    if not os.path.exists(PROFILE_TRAFFIC):
+        return None
+    for line in open(PROFILE_TRAFFIC):
+        if line.strip().startswith(key + ":"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
 def profiled_traffic():
     """DRAM bytes per launch of the stencil kernel from the committed ncu
     summary (a line `traffic_bytes_per_launch: N`), or None."""
@@ -322,6 +336,19 @@ def run_ours(args, rank, world, local_rank):
         print(f"peak probes failed: {exc}", file=sys.stderr)
         pk = None
     onchip = onchip_rooflines(pr, cc_per_sweep / (ms / 1000.0), 4, pk)
+    # the binding ceiling: instruction issue (4 warp schedulers per SM, one
+    # instruction each per clock, at the SM clock sampled during the timing)
+    wipu = profiled_value("warp_instructions_per_update")
+    clk_mhz = (clk.summary() or {}).get("sm_mhz")
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    if wipu and clk_mhz:
+        issued = cc_per_sweep / (ms / 1000.0) * wipu
+        peak_issue = sms * 4 * clk_mhz * 1e6
+        onchip["issue"] = {"achieved": issued, "peak": peak_issue, "unit": "warp instructions/s",
+                           "frac": issued / peak_issue,
+                           "instructions_per_update": wipu,
+                           "peak_source": f"{sms} SMs x 4 schedulers x {clk_mhz:.0f} MHz (sampled)",
+                           "instructions_source": "ncu summary in profiles/"}
 
     # ---- CPU baseline: the oracle on the host cores, bounded sample
     from oracle import oracle as og
