@@ -283,7 +283,8 @@ typedef struct pg_adjoint_result {
  * its current (converged) FP32 table, given dl_dv = dL/dV (ncells floats,
  * row-major; a device pointer when dl_dv_on_device, else host).  The policy
  * is the table's argmin (one extra sweep that leaves V unchanged); the
- * adjoint lambda = dL/dV + P^T lambda is iterated until its L1 change is at
+ * adjoint lambda = dL/dV + P^T lambda is iterated (in FP64; 16 bytes of
+ * device memory per cell for the two iterates) until its L1 change is at
  * most tol * |dL/dV|_1 or `iters` sweeps ran.  Plain scheme with the masked
  * stencil's records only (PG_EUNSUPPORTED otherwise).  No counterpart in
  * the reference, which never differentiates its tables. */

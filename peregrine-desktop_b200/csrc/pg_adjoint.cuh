@@ -283,8 +283,10 @@ __global__ void k_adj_active(const float* __restrict__ V, const int16_t* __restr
 
 // lambda_out += P^T lambda_in over the active cells (lambda_out holds c on
 // entry).  Grid-stride over the cells; 64 atomic adds per active cell with
-// a nonzero lambda.
-__global__ void k_adj_scatter(const float* __restrict__ lam_in, float* __restrict__ lam_out,
+// a nonzero lambda.  lambda is FP64: the order of the atomic adds changes
+// from sweep to sweep, and in FP32 that reordering alone moves |dlambda|_1
+// by ~1e-5 of |c|_1, a floor the stop rule could not get under.
+__global__ void k_adj_scatter(const double* __restrict__ lam_in, double* __restrict__ lam_out,
                               const int16_t* __restrict__ pol, const uint8_t* __restrict__ active,
                               const uint32_t* __restrict__ recs, KParams kp) {
     const Layout L = make_layout(kp);
@@ -292,8 +294,8 @@ __global__ void k_adj_scatter(const float* __restrict__ lam_in, float* __restric
     load_grid(g, kp.g);
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < kp.ncells;
          e += (int64_t)gridDim.x * blockDim.x) {
-    const float lv = lam_in[e];
-    if (lv == 0.0f || !active[e]) continue;
+    const double lv = lam_in[e];
+    if (lv == 0.0 || !active[e]) continue;
     const int64_t pl = e / L.P;
     const int32_t r = (int32_t)(e - pl * L.P);
     const int32_t i = r / L.n[1], j = r - i * L.n[1];
@@ -311,23 +313,41 @@ __global__ void k_adj_scatter(const float* __restrict__ lam_in, float* __restric
     const float wxy[4] = {(1.0f - tx) * (1.0f - ty), tx * (1.0f - ty), (1.0f - tx) * ty, tx * ty};
     const int32_t off[4] = {r0 * L.n[1] + c0, r1 * L.n[1] + c0, r0 * L.n[1] + c1, r1 * L.n[1] + c1};
     for (int c = 0; c < 16; ++c) {
-        const float w = __uint_as_float(rec[c]) * lv;
-        if (w == 0.0f) continue;
-        float* dst = lam_out + (int64_t)rec[kUNT + c] * L.P;
+        const double w = (double)__uint_as_float(rec[c]) * lv;
+        if (w == 0.0) continue;
+        double* dst = lam_out + (int64_t)rec[kUNT + c] * L.P;
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-            if (wxy[q] != 0.0f) atomicAdd(dst + off[q], w * wxy[q]);
+            if (wxy[q] != 0.0f) atomicAdd(dst + off[q], w * (double)wxy[q]);
     }
     }
 }
 
-// sum |a - b| into per-block partials (the adjoint's convergence signal)
-__global__ void k_adj_diff(const float* __restrict__ a, const float* __restrict__ b, int64_t n,
-                           double* part_sum, double* part_max) {
+// lambda_0 = lambda_1 = c, and |c|_1 into per-block partials
+__global__ void k_adj_start(const float* __restrict__ c, double* __restrict__ l0,
+                            double* __restrict__ l1, int64_t n, double* part_sum, double* part_max) {
     double s = 0.0, m = 0.0;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
          k += (int64_t)gridDim.x * blockDim.x) {
-        const double d = fabs((double)a[k] - (double)b[k]);
+        const double v = (double)c[k];
+        l0[k] = v;
+        l1[k] = v;
+        s += fabs(v);
+        m = fmax(m, fabs(v));
+    }
+    block_partial(s, m, part_sum, part_max);
+}
+
+// sum |lout - lin| into per-block partials (the adjoint's convergence
+// signal), then lin = c: lin is the next sweep's output and starts from c
+__global__ void k_adj_step(const double* __restrict__ lout, double* __restrict__ lin,
+                           const float* __restrict__ c, int64_t n, double* part_sum,
+                           double* part_max) {
+    double s = 0.0, m = 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const double d = fabs(lout[k] - lin[k]);
+        lin[k] = (double)c[k];
         s += d;
         m = fmax(m, d);
     }
@@ -355,7 +375,7 @@ __host__ __device__ inline size_t adj_grad_smem(int nctl) {
 // fractions, exactly as the forward sweep) and the dual successor; phase B
 // walks the plane's cells.  The 18 sums go to `grad` with double atomics.
 __global__ void __launch_bounds__(128)
-    k_adj_grad(const float* __restrict__ V, const float* __restrict__ lam,
+    k_adj_grad(const float* __restrict__ V, const double* __restrict__ lam,
                const int16_t* __restrict__ pol, const uint8_t* __restrict__ active,
                const uint32_t* __restrict__ recs, KParams kp, const float* __restrict__ ctl,
                double* __restrict__ grad) {
@@ -379,7 +399,7 @@ __global__ void __launch_bounds__(128)
     // any work in this plane?
     int any = 0;
     for (int64_t k = threadIdx.x; k < P; k += blockDim.x)
-        any |= (active[pl * P + k] && lam[pl * P + k] != 0.0f);
+        any |= (active[pl * P + k] && lam[pl * P + k] != 0.0);
     if (!__syncthreads_or(any)) return;
 
     for (int u = threadIdx.x; u < nctl; u += blockDim.x) {
@@ -413,8 +433,8 @@ __global__ void __launch_bounds__(128)
     for (int64_t k = threadIdx.x; k < P; k += blockDim.x) {
         const int64_t e = pl * P + k;
         if (!active[e]) continue;
-        const float lv = lam[e];
-        if (lv == 0.0f) continue;
+        const float lv = (float)lam[e];
+        if (lam[e] == 0.0) continue;
         const int32_t i = (int32_t)(k / L.n[1]), j = (int32_t)(k - (int64_t)i * L.n[1]);
         const int u = pol[L.rowmajor(i, j, i3, i4, i5, i6)];
         if (!sok[4 * u]) continue;

@@ -793,7 +793,7 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
     const int64_t n = kp.ncells;
     if (!ctx->argmin_d)
         PG_CUDA(cudaMalloc(&ctx->argmin_d, (size_t)n * sizeof(int16_t)));
-    float* lam[2] = {nullptr, nullptr};
+    double* lam[2] = {nullptr, nullptr};
     float* c = nullptr;
     uint8_t* active = nullptr;
     double* grad_d = nullptr;
@@ -809,8 +809,8 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
         return fail(e == cudaErrorMemoryAllocation ? PG_ENOMEM : PG_ECUDA,
                     std::string(what) + ": " + cudaGetErrorString(e));
     };
-    cudaError_t e = cudaMalloc(&lam[0], (size_t)n * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&lam[1], (size_t)n * 4);
+    cudaError_t e = cudaMalloc(&lam[0], (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&lam[1], (size_t)n * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&c, (size_t)n * 4);
     if (e == cudaSuccess) e = cudaMalloc(&active, (size_t)n);
     if (e == cudaSuccess) e = cudaMalloc(&grad_d, pg::kNThetaHost * sizeof(double));
@@ -852,27 +852,24 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
     if (e != cudaSuccess) return cuda_fail(e, "adjoint set-up");
     rc = read_residual(ctx, &nact, &dm0);
     if (rc) { release(); return rc; }
-    if (e == cudaSuccess) e = cudaMemsetAsync(lam[1], 0, (size_t)n * 4, ctx->stream);
-    if (e == cudaSuccess) e = pg::launch_adj_diff(c, lam[1], n, sb, ctx->stream);
+    // lambda_0 = c, and the first sweep's output starts from c
+    if (e == cudaSuccess) e = pg::launch_adj_start(c, lam[0], lam[1], n, sb, ctx->stream);
     ctx->launches += 2;
     if (e != cudaSuccess) return cuda_fail(e, "adjoint set-up");
     double cn = 0.0, dm = 0.0;
     rc = read_residual(ctx, &cn, &dm);
     if (rc) { release(); return rc; }
 
-    // lambda <- c + P^T lambda until quiet
-    e = cudaMemcpyAsync(lam[0], c, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "adjoint set-up");
+    // lambda <- c + P^T lambda until quiet; the step kernel measures the
+    // change and resets the older buffer to c for the next sweep
     int cur = 0, done = 0;
     double r = INFINITY, kms = 0.0;
     for (int32_t it = 1; it <= iters && cn > 0.0; ++it) {
-        float* lin = lam[cur];
-        float* lout = lam[1 - cur];
+        double* lin = lam[cur];
+        double* lout = lam[1 - cur];
         PG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-        e = cudaMemcpyAsync(lout, c, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
-        if (e == cudaSuccess)
-            e = pg::launch_adj_scatter(lin, lout, ctx->argmin_d, active, ctx->recs_d, kp, ctx->stream);
-        if (e == cudaSuccess) e = pg::launch_adj_diff(lout, lin, n, sb, ctx->stream);
+        e = pg::launch_adj_scatter(lin, lout, ctx->argmin_d, active, ctx->recs_d, kp, ctx->stream);
+        if (e == cudaSuccess) e = pg::launch_adj_step(lout, lin, c, n, sb, ctx->stream);
         ctx->launches += 3;
         if (e != cudaSuccess) return cuda_fail(e, "adjoint sweep");
         PG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));

@@ -1051,17 +1051,25 @@ cudaError_t launch_adj_active(const float* V, const int16_t* pol, const uint8_t*
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_scatter(const float* lam_in, float* lam_out, const int16_t* pol,
+cudaError_t launch_adj_scatter(const double* lam_in, double* lam_out, const int16_t* pol,
                                const uint8_t* active, const uint32_t* recs, const KParams& kp,
                                cudaStream_t st) {
     k_adj_scatter<<<grid_for(kp.ncells, 256), 256, 0, st>>>(lam_in, lam_out, pol, active, recs, kp);
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_diff(const float* a, const float* b, int64_t n, const SweepBufs& sb,
-                            cudaStream_t st) {
+cudaError_t launch_adj_start(const float* c, double* l0, double* l1, int64_t n, const SweepBufs& sb,
+                             cudaStream_t st) {
     const int64_t blocks = std::min<int64_t>(sb.nparts, 148 * 16);
-    k_adj_diff<<<(unsigned)blocks, 256, 0, st>>>(a, b, n, sb.part_sum, sb.part_max);
+    k_adj_start<<<(unsigned)blocks, 256, 0, st>>>(c, l0, l1, n, sb.part_sum, sb.part_max);
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_step(const double* lout, double* lin, const float* c, int64_t n,
+                            const SweepBufs& sb, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(sb.nparts, 148 * 16);
+    k_adj_step<<<(unsigned)blocks, 256, 0, st>>>(lout, lin, c, n, sb.part_sum, sb.part_max);
     k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
     return cudaGetLastError();
 }
@@ -1073,7 +1081,7 @@ cudaError_t launch_adj_count(const uint8_t* a, int64_t n, const SweepBufs& sb, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_grad(const float* V, const float* lam, const int16_t* pol,
+cudaError_t launch_adj_grad(const float* V, const double* lam, const int16_t* pol,
                             const uint8_t* active, const uint32_t* recs, const KParams& kp,
                             const float* ctl, double* grad, cudaStream_t st) {
     const size_t smem = adj_grad_smem(kp.nctl);

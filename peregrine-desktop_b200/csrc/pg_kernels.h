@@ -55,13 +55,15 @@ int batch_blocks_per_sm(int storage, size_t smem, int threads);
 cudaError_t launch_adj_active(const float* V, const int16_t* pol, const uint8_t* occ,
                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                               uint8_t* active, cudaStream_t st);
-cudaError_t launch_adj_scatter(const float* lam_in, float* lam_out, const int16_t* pol,
+cudaError_t launch_adj_scatter(const double* lam_in, double* lam_out, const int16_t* pol,
                                const uint8_t* active, const uint32_t* recs, const KParams& kp,
                                cudaStream_t st);
-cudaError_t launch_adj_diff(const float* a, const float* b, int64_t n, const SweepBufs& sb,
-                            cudaStream_t st);
+cudaError_t launch_adj_start(const float* c, double* l0, double* l1, int64_t n, const SweepBufs& sb,
+                             cudaStream_t st);
+cudaError_t launch_adj_step(const double* lout, double* lin, const float* c, int64_t n,
+                            const SweepBufs& sb, cudaStream_t st);
 cudaError_t launch_adj_count(const uint8_t* a, int64_t n, const SweepBufs& sb, cudaStream_t st);
-cudaError_t launch_adj_grad(const float* V, const float* lam, const int16_t* pol,
+cudaError_t launch_adj_grad(const float* V, const double* lam, const int16_t* pol,
                             const uint8_t* active, const uint32_t* recs, const KParams& kp,
                             const float* ctl, double* grad, cudaStream_t st);
 size_t stencil_u_smem_bytes(const KParams& kp);

@@ -3,8 +3,10 @@ against an independent CPU FP64 reference and against central finite
 differences of FP64 solves.  The loss is the mean table value over start
 states at rest, as in the differentiation benchmark.
 
-Tolerances: the GPU adjoint accumulates lambda in FP32 with atomic adds, so
-its gradient carries ~1e-5 relative noise; the CPU reference (FP64, finite-
+Tolerances: the GPU adjoint accumulates lambda in FP64 with atomic adds (in
+an order that changes from sweep to sweep, so FP32 would leave a residual
+floor near 1e-5 of |c|_1) and the 18 sums per block in FP32, so its gradient
+carries ~1e-5 relative noise; the CPU reference (FP64, finite-
 difference successor derivatives) agrees within 1e-4 of the largest entry.
 Finite differences of full solves (relative step 1e-3) also see the
 policy's switches between neighbouring controls; 1e-3 of the largest entry
