@@ -107,6 +107,10 @@ typedef struct pg_params {
 #define PG_KERNEL_STENCIL_EXACT 3 /* stencil with the reference's rounding order */
 #define PG_KERNEL_STENCIL_ROWS  4 /* stencil deciding every probe per sweep (no mask) */
 #define PG_KERNEL_STENCIL_GATHER 5 /* masked stencil gathering all 64 corners per cell */
+#define PG_KERNEL_STENCIL_BLEND  6 /* masked stencil, blend-then-shift re-reading the
+                                      corner planes per control (PG_KERNEL_STENCIL runs
+                                      the register-resident blend where it fits; both
+                                      give bit-identical tables) */
 
 /* Table dtypes (solver/src/Pipeline.jl:620-625). */
 #define PG_DTYPE_U8  0
@@ -217,9 +221,12 @@ int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
 /* Number of this library's kernel launches since the context was created. */
 int pg_launch_count(pg_ctx* ctx, int64_t* launches);
 
-/* Rows of one plane per block of the blend-then-shift sweep (the tile
- * shape the autotuner picks): 1 <= rows <= Nx and rows * Ny <= 1024.  No
- * counterpart in the reference (its kernel has one thread per cell). */
+/* Rows of one plane per block of the blend-then-shift sweeps (the tile
+ * shape the autotuner picks): 1 <= rows <= Nx, and rows * Ny <= 1024 (the
+ * re-reading blend) or (rows + 3) * Ny <= 2048 (the register-resident blend,
+ * whose window has 3 more rows); a kernel whose limit the rows exceed is not
+ * used.  No counterpart in the reference (its kernel has one thread per
+ * cell). */
 int pg_set_tile_rows(pg_ctx* ctx, int32_t rows);
 
 /* ------------------------------------------------------------------ */

@@ -84,6 +84,8 @@ struct pg_ctx {
     bool mask_ok = false;
     bool blend_ok = false;   // the blend-then-shift tiling fits (shared memory, row width)
     bool gather_ok = false;  // the 64-corner masked gather fits its shared memory
+    uint16_t* gord_d = nullptr;  // per plane, its controls in corner-group order
+    bool rblend_ok = false;      // the register-resident blend can run (gord_d, tiling)
     int8_t* pol_d = nullptr;
     double* part_sum = nullptr;
     double* part_max = nullptr;
@@ -119,6 +121,9 @@ struct pg_ctx {
         mask_ok = false;
         blend_ok = false;
         gather_ok = false;
+        if (gord_d) cudaFree(gord_d);
+        gord_d = nullptr;
+        rblend_ok = false;
         if (pol_d) cudaFree(pol_d);
         if (part_sum) cudaFree(part_sum);
         if (part_max) cudaFree(part_max);
@@ -174,15 +179,51 @@ int ensure_values(pg_ctx* ctx, int storage) {
     return PG_OK;
 }
 
+// Register-resident blend tiling: the window ((rows + 3) x Ny cells) takes
+// kRCellsPerThread cells per thread, at most 2048 cells.  rows = 0 picks: the
+// most rows whose window fits 1024 cells (two blocks per SM) when the three
+// extra window rows cost at most a quarter, else the most that fit 2048,
+// balanced over the plane; rows < 0 or a window that does not fit leaves the
+// tiling at 0 (not eligible).
+void r_tiling(pg::KParams& kp, int32_t rows) {
+    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
+    kp.rtile_x = kp.rtiles_x = kp.rblock = 0;
+    if (rows < 0 || n2 < 1 || n2 > 0xffff) return;
+    int32_t tx = rows;
+    if (tx <= 0) {
+        const int32_t t1 = std::min<int32_t>(n1, 1024 / n2 - 3);
+        const int32_t t2 = std::min<int32_t>(n1, 2048 / n2 - 3);
+        tx = (t1 >= 1 && (t1 == n1 || 4 * (t1 + 3) <= 5 * t1)) ? t1 : t2;
+        if (tx < 1) return;
+        const int32_t nt = (n1 + tx - 1) / tx;
+        tx = (n1 + nt - 1) / nt;
+    }
+    const int64_t win = (int64_t)(tx + 3) * n2;
+    if (tx < 1 || tx > n1 || win > pg::kRMaxWindowHost) return;
+    kp.rtile_x = tx;
+    kp.rtiles_x = (n1 + tx - 1) / tx;
+    const int64_t kc = pg::kRCellsPerThread;
+    kp.rblock = (int32_t)std::max<int64_t>(64, 32 * (((win + kc - 1) / kc + 31) / 32));
+}
+
+// The register-resident blend keeps every control's successor corners in
+// shared memory; it runs where that leaves room for two blocks per SM (or,
+// with more than 256 threads, the block has the SM to itself anyway) and the
+// re-reading blend runs elsewhere.
+bool r_smem_fits(const pg::KParams& kp) {
+    return kp.rtile_x > 0 &&
+           pg::stencil_r_smem_bytes(kp) <= (size_t)(kp.rblock > 256 ? 200 : 100) * 1024;
+}
+
 int pick_kernel(pg_ctx* ctx, int32_t kernel, int* out) {
     if (kernel == PG_KERNEL_AUTO) kernel = ctx->stencil_ok ? PG_KERNEL_STENCIL : PG_KERNEL_CELLFORM;
     if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_EXACT) && !ctx->stencil_ok)
         return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
     if (kernel == PG_KERNEL_STENCIL_ROWS && !ctx->stencil_ok)
         return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
-    if (kernel == PG_KERNEL_STENCIL_GATHER && !ctx->stencil_ok)
+    if ((kernel == PG_KERNEL_STENCIL_GATHER || kernel == PG_KERNEL_STENCIL_BLEND) && !ctx->stencil_ok)
         return fail(PG_EUNSUPPORTED, "the stencil kernel cannot run this scheme: " + ctx->stencil_why);
-    if (kernel < PG_KERNEL_STENCIL || kernel > PG_KERNEL_STENCIL_GATHER)
+    if (kernel < PG_KERNEL_STENCIL || kernel > PG_KERNEL_STENCIL_BLEND)
         return fail(PG_EINVAL, "unknown kernel " + std::to_string(kernel));
     *out = kernel;
     return PG_OK;
@@ -196,15 +237,24 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
     const void* vin = ctx->V[ctx->cur];
     void* vout = ctx->V[1 - ctx->cur];
     cudaError_t e;
+    const bool r_ok = ctx->mask_ok && ctx->rblend_ok && ctx->storage != PG_STORE_F64;
+    const bool b_ok = ctx->mask_ok && ctx->blend_ok && ctx->storage != PG_STORE_F64;
     if (ctx->storage == PG_STORE_Q16 &&
-        (esc || kernel != PG_KERNEL_STENCIL || !ctx->mask_ok || !ctx->blend_ok))
-        return fail(PG_EUNSUPPORTED, "Q16 storage is swept by the blend-then-shift kernel only");
+        (esc || !((kernel == PG_KERNEL_STENCIL && (r_ok || b_ok)) ||
+                  (kernel == PG_KERNEL_STENCIL_BLEND && b_ok))))
+        return fail(PG_EUNSUPPORTED, "Q16 storage is swept by the blend-then-shift kernels only");
+    if (kernel == PG_KERNEL_STENCIL_BLEND && !esc && !b_ok)
+        return fail(PG_EUNSUPPORTED, "the blend-then-shift kernel cannot run this table (its "
+                                     "tiling, shared memory, or FP64 storage)");
     if (esc || kernel == PG_KERNEL_CELLFORM)
         e = pg::launch_cellform(ctx->storage, esc, vin, vout, ctx->occ_d,
                                 use_pol ? ctx->pol_d : nullptr, ctx->kp, ctx->ctl_d, sb, argmin_d,
                                 ctx->stream, &ctx->launches);
-    else if (kernel == PG_KERNEL_STENCIL && ctx->mask_ok && ctx->blend_ok &&
-             ctx->storage != PG_STORE_F64)
+    else if (kernel == PG_KERNEL_STENCIL && r_ok)
+        e = pg::launch_stencil_r(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
+                                 ctx->kp, ctx->gord_d, sb, argmin_d, ctx->stream,
+                                 &ctx->launches);
+    else if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_BLEND) && b_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  ctx->kp, ctx->order_d, sb, argmin_d, ctx->stream,
                                  &ctx->launches);
@@ -435,6 +485,7 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
         kp.btiles_x = nt;
         kp.bblock = (int32_t)th;
     }
+    r_tiling(kp, 0);
     kp.nsub = host_substeps_for(p->cfl <= 0.0f ? p->dt : p->tau_max, *p);
     kp.nchk = p->checks;
 
@@ -495,6 +546,8 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     if (ub > ctx->nparts) ctx->nparts = ub;
     const int64_t bb = kp.nplanes * kp.btiles_x;
     if (bb > ctx->nparts) ctx->nparts = bb;
+    const int64_t rb = kp.nplanes * kp.rtiles_x;
+    if (rb > ctx->nparts) ctx->nparts = rb;
     PG_CUDA(cudaMalloc(&ctx->part_sum, sizeof(double) * ctx->nparts));
     PG_CUDA(cudaMalloc(&ctx->part_max, sizeof(double) * ctx->nparts));
     // The admissibility mask of the masked stencil: decided once here, read by
@@ -512,6 +565,19 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
             ctx->mask_ok = true;
             ctx->blend_ok = kp.btile_x > 0 && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
             ctx->gather_ok = pg::stencil_u_smem_bytes(kp) <= 200 * 1024;
+            // the register-resident blend's per-plane control order
+            if (kp.rtile_x > 0 && kp.nctl <= 0x7fff && r_smem_fits(kp) &&
+                cudaMalloc(&ctx->gord_d, (size_t)kp.nplanes * kp.nctl * sizeof(uint16_t)) ==
+                    cudaSuccess) {
+                e = pg::launch_stencil_group(ctx->recs_d, kp, ctx->order_d, ctx->gord_d,
+                                             ctx->stream, &ctx->launches);
+                if (e != cudaSuccess)
+                    return fail(PG_ECUDA, std::string("group: ") + cudaGetErrorString(e));
+                ctx->rblend_ok = true;
+            } else {
+                cudaGetLastError();
+                ctx->gord_d = nullptr;
+            }
         } else {
             cudaGetLastError();
             if (ctx->mask_d) cudaFree(ctx->mask_d);
@@ -820,7 +886,10 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
     pg::SweepBufs sb{ctx->part_sum, ctx->part_max, ctx->nparts, ctx->red_d};
     const void* vin = ctx->V[ctx->cur];
     void* spare = ctx->V[1 - ctx->cur];
-    if (ctx->blend_ok)
+    if (ctx->rblend_ok)
+        e = pg::launch_stencil_r(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
+                                 kp, ctx->gord_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
+    else if (ctx->blend_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  kp, ctx->order_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
     else if (ctx->gather_ok)
@@ -911,8 +980,11 @@ int pg_set_tile_rows(pg_ctx* ctx, int32_t rows) {
     if (rc) return rc;
     pg::KParams& kp = ctx->kp;
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
-    if (rows < 1 || rows > n1 || (int64_t)rows * n2 > pg::kBMaxTileCells)
-        return fail(PG_EINVAL, "tile rows must be in [1, Nx] with rows * Ny <= 1024");
+    const bool b_fits = (int64_t)rows * n2 <= pg::kBMaxTileCells;
+    const bool r_fits = (int64_t)(rows + 3) * n2 <= pg::kRMaxWindowHost;
+    if (rows < 1 || rows > n1 || !(b_fits || r_fits))
+        return fail(PG_EINVAL, "tile rows must be in [1, Nx] with rows * Ny <= 1024 or "
+                               "(rows + 3) * Ny <= 2048");
     const int32_t nt = (n1 + rows - 1) / rows;
     const int64_t need = kp.nplanes * nt;
     if (need > ctx->nparts) {
@@ -929,13 +1001,19 @@ int pg_set_tile_rows(pg_ctx* ctx, int32_t rows) {
         ctx->part_max = pm;
         ctx->nparts = need;
     }
-    const int64_t cells = (int64_t)rows * n2;
-    int64_t th = 32 * (((cells + 2) / 3 + 31) / 32);
-    th = std::max<int64_t>(64, std::min<int64_t>(256, th));
-    kp.btile_x = rows;
-    kp.btiles_x = nt;
-    kp.bblock = (int32_t)th;
-    ctx->blend_ok = ctx->mask_ok && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
+    if (b_fits) {
+        const int64_t cells = (int64_t)rows * n2;
+        int64_t th = 32 * (((cells + 2) / 3 + 31) / 32);
+        th = std::max<int64_t>(64, std::min<int64_t>(256, th));
+        kp.btile_x = rows;
+        kp.btiles_x = nt;
+        kp.bblock = (int32_t)th;
+    } else {
+        kp.btile_x = kp.btiles_x = kp.bblock = 0;
+    }
+    ctx->blend_ok = ctx->mask_ok && b_fits && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
+    r_tiling(kp, r_fits ? rows : -1);
+    ctx->rblend_ok = ctx->gord_d && kp.rtile_x > 0 && r_smem_fits(kp);
     return PG_OK;
 }
 

@@ -575,6 +575,7 @@ __global__ void __launch_bounds__(kCellThreads)
 #include "pg_stencil.cuh"
 #include "pg_stencil_u.cuh"
 #include "pg_stencil_b.cuh"
+#include "pg_stencil_r.cuh"
 #include "pg_adjoint.cuh"
 
 // ---------------------------------------------------------------------------
@@ -1037,6 +1038,80 @@ int batch_blocks_per_sm(int storage, size_t smem, int threads) {
         case PG_STORE_Q16: return batch_occupancy<Q16>(threads, smem);
     }
     return 0;
+}
+
+cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const int32_t* order,
+                                 uint16_t* gord, cudaStream_t st, int64_t* launches) {
+    const size_t smem = stencil_group_smem(kp.nctl);
+    if (smem > 200 * 1024 || kp.nplanes > 0x7fffffffLL || kp.nctl > 0x7fff)
+        return cudaErrorInvalidValue;
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set & attr_bit)) {
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_group,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set |= attr_bit;
+    }
+    k_stencil_group<<<(unsigned)kp.nplanes, 128, smem, st>>>(recs, kp, order, gord);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+template <typename S, bool ARGMIN, int KR>
+static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
+                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                               const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
+                               cudaStream_t st, int64_t* launches) {
+    if (kp.rtile_x <= 0 || kp.rblock <= 0 || kp.rblock > RShape<KR>::kMaxThreads ||
+        kp.rblock % 32 != 0 || kp.nsub > kStencilMaxSub || kp.g.n[1] > 0xffff ||
+        (int64_t)(kp.rtile_x + 3) * kp.g.n[1] > (int64_t)kp.rblock * KR)
+        return cudaErrorInvalidValue;
+    KParams kr = kp;
+    kr.tile_x = kp.rtile_x;
+    kr.tiles_x = kp.rtiles_x;
+    const int64_t blocks = kp.nplanes * kp.rtiles_x;
+    if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const size_t smem = stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1]);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set & attr_bit)) {
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_r<S, ARGMIN, KR>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set |= attr_bit;
+    }
+    k_stencil_r<S, ARGMIN, KR><<<(unsigned)blocks, kp.rblock, smem, st>>>(
+        (const S*)Vin, (S*)Vout, occ, mask, recs, kr, gord, sb.part_sum, sb.part_max, argmin);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uint8_t* occ,
+                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                             const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
+                             cudaStream_t st, int64_t* launches) {
+#define PG_SR(S)                                                                                 \
+    return argmin ? stencil_r_t<S, true, kRCellsPerThread>(Vin, Vout, occ, mask, recs, kp, gord, \
+                                                           sb, argmin, st, launches)             \
+                  : stencil_r_t<S, false, kRCellsPerThread>(Vin, Vout, occ, mask, recs, kp,      \
+                                                            gord, sb, argmin, st, launches)
+    switch (storage) {
+        case PG_STORE_F32: PG_SR(float);
+        case PG_STORE_F16: PG_SR(__half);
+        case PG_STORE_BF16: PG_SR(__nv_bfloat16);
+        case PG_STORE_Q16: PG_SR(Q16);
+    }
+#undef PG_SR
+    return cudaErrorInvalidValue;
+}
+
+size_t stencil_r_smem_bytes(const KParams& kp) {
+    return stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1]);
 }
 
 size_t stencil_b_smem_bytes(const KParams& kp) {

@@ -81,17 +81,23 @@ template <> struct BUnpack<Q16> {
 };
 
 // Shared memory of one block: two record slots, the control order, two
-// window buffers and two sets of per-row / per-column successor corners.
+// window buffers, two sets of per-row / per-column successor corners and
+// three slots of the tile's admissibility-mask rows.
 __host__ __device__ inline size_t stencil_b_smem(int nctl, int tile_x, int n2) {
     return 2 * (size_t)kURec * 4 + (size_t)((nctl + 3) & ~3) * 4 +
            2 * (size_t)(tile_x + 3) * n2 * sizeof(float) +
-           2 * (size_t)(tile_x + n2) * 2 * sizeof(int32_t);
+           2 * (size_t)(tile_x + n2) * 2 * sizeof(int32_t) +
+           3 * (size_t)tile_x * mask_words(n2) * sizeof(uint32_t);
 }
 
 // 16-byte global -> shared copy that completes asynchronously (cp.async).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
     asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -125,6 +131,11 @@ __device__ __forceinline__ void stencil_b_item(
     // column, y fraction) of each column, double-buffered like the window
     int2* rinfo = reinterpret_cast<int2*>(Bbuf + 2 * bsz);
     int2* cinfo = rinfo + 2 * TX;
+    // per control: the tile rows of its admissibility mask, three slots --
+    // the prefetch for control uu+1 must not overwrite the slot that a
+    // thread still in control uu-1's phase 2 reads
+    uint32_t* mslot = reinterpret_cast<uint32_t*>(cinfo + 2 * n2);
+    const int32_t mstride = TX * W;
     const Layout L = make_layout(kp);
     GridT<float> g;
     load_grid(g, kp.g);
@@ -165,11 +176,17 @@ __device__ __forceinline__ void stencil_b_item(
         if (e < ncell && occ_h[e] == 0) live |= 1u << q;
     }
     const uint32_t* mplane = mask + ((size_t)pl * nctl * n1 + x0) * W;
+    const int32_t nmw = nr * W;  // mask words of the tile per control
+    // mask words are copied by the threads after the first warp (which
+    // copies the record)
+    const int32_t mt = tid >= 32 ? tid - 32 : tid + T - 32;
     for (int i = tid; i < nctl; i += T) ord[i] = __ldg(order + i);
     __syncthreads();
     constexpr int kRecVec = kURec / 4;  // 16-byte pieces of a record
     if (tid < kRecVec)
         cp_async16(rslot + 4 * tid, prec + (size_t)ord[0] * kURec + 4 * tid);
+    for (int32_t k = mt; k < nmw; k += T)
+        cp_async4(mslot + k, mplane + (size_t)ord[0] * n1 * W + k);
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
@@ -180,9 +197,16 @@ __device__ __forceinline__ void stencil_b_item(
         const uint32_t* rec = rslot + (uu & 1) * kURec;
         // prefetch the next control's record into the other slot; it is
         // waited for at this control's barrier
-        if (uu + 1 < nctl && tid < kRecVec)
-            cp_async16(rslot + ((uu + 1) & 1) * kURec + 4 * tid,
-                       prec + (size_t)ord[uu + 1] * kURec + 4 * tid);
+        const int ms = uu % 3;
+        if (uu + 1 < nctl) {
+            const int un = ord[uu + 1];
+            if (tid < kRecVec)
+                cp_async16(rslot + ((uu + 1) & 1) * kURec + 4 * tid,
+                           prec + (size_t)un * kURec + 4 * tid);
+            uint32_t* md = mslot + (ms == 2 ? 0 : ms + 1) * mstride;
+            const uint32_t* msrc = mplane + (size_t)un * n1 * W;
+            for (int32_t k = mt; k < nmw; k += T) cp_async4(md + k, msrc + k);
+        }
         cp_async_commit();
         // (ox, oy, ok, nsub)
         const int4 oi = *reinterpret_cast<const int4*>(rec + kUNT + 16);
@@ -289,13 +313,13 @@ __device__ __forceinline__ void stencil_b_item(
 
         // phase 2: shift, admissibility, tau, min (the record slot is not
         // read here: the next prefetch may already be filling it)
-        const uint32_t* mctl = mplane + (size_t)u * n1 * W;
+        const uint32_t* mctl = mslot + ms * mstride;
 #pragma unroll
         for (int q = 0; q < kBCells; ++q) {
             if (tid + q * T >= ncell) break;
             float cv = cap;
             const bool adm =
-                ((live >> q) & 1u) && ((__ldg(mctl + cm[q]) >> (cj[q] & 31)) & 1u);
+                ((live >> q) & 1u) && ((mctl[cm[q]] >> (cj[q] & 31)) & 1u);
             if (adm) {
                 const int2 rr = ri[ca[q]];
                 const int2 cc = ci[cj[q]];

@@ -1,0 +1,373 @@
+// pg_stencil_r.cuh -- the plain scheme's sweep as blend-then-shift with the
+// corner planes held in registers (included inside namespace pg by
+// pg_kernels.cu, after pg_stencil_b.cuh, whose records, mask, shared-memory
+// helpers and storage unpacking it shares).
+//
+// k_stencil_b re-reads the 16 corner planes of every control from L2.  But
+// the controls of one destination plane land on very few distinct corner
+// sets: the successor's (h, v) moves by at most a cell or two over one
+// lookahead, so the 125 controls of the benchmark grid fall into about two
+// groups that share the same 16 corner planes and the same nominal x offset
+// (and about 23 distinct planes in all, against 2000 plane reads).  So:
+//
+//   k_stencil_group (once per solve) sorts each plane's controls by their
+//   (corner planes, x offset) and flags the first control of each group;
+//   controls that no cell of the plane admits go last;
+//
+//   k_stencil_r loads, at the first control of each group, the 16 corner
+//   values of each of its window cells into registers (KR cells per thread),
+//   and for every control of the group blends them with the control's 16
+//   weights -- 16 FMAs per window cell from registers, nothing re-read --
+//   into the shared window, then shifts exactly as k_stencil_b does.
+//
+// The arithmetic is k_stencil_b's, operation for operation: the same FMA
+// chain over the corners in record order, the same per-row / per-column
+// successor corners and fractions, the same bilinear step; the results are
+// bit-identical to it.  The window has one padding column (a copy of the
+// last column), so the upper column corner needs no clamp.
+
+// Controls of a plane in group order: entry = control | kGroupFirst on the
+// first control of a group.
+constexpr uint16_t kGroupFirst = 0x8000u;
+constexpr int kRMaxWindow = 2048;  // window cells per block
+
+// Threads per block at most and the minimum resident blocks for KR window
+// cells per thread: 16 KR corner registers per thread, so KR = 2 keeps 64
+// registers and up to 1024 threads; KR = 4, 128 registers and 512 threads.
+template <int KR> struct RShape;
+template <> struct RShape<2> { static constexpr int kMaxThreads = 1024, kMinBlocks = 1; };
+template <> struct RShape<4> { static constexpr int kMaxThreads = 512, kMinBlocks = 1; };
+
+__host__ __device__ inline size_t stencil_group_smem(int nctl) {
+    return (size_t)nctl * (17 * sizeof(int32_t) + 2 * sizeof(int32_t));
+}
+
+// Block = plane.  Key of a control: (not admissible anywhere, its 16 corner
+// planes, its x offset); rank = number of controls with a smaller key, or
+// the same key and an earlier place in `order` (the (u1, u2, u3) order).
+__global__ void __launch_bounds__(128)
+    k_stencil_group(const uint32_t* __restrict__ recs, KParams kp, const int32_t* __restrict__ order,
+                    uint16_t* __restrict__ gord) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nctl = kp.nctl;
+    int32_t* key = reinterpret_cast<int32_t*>(smem_raw);  // [nctl][17]: planes, ox
+    int32_t* pos = key + (size_t)nctl * 17;               // [nctl] place in order
+    int32_t* srt = pos + nctl;                            // [nctl] sorted controls
+    const int64_t pl = blockIdx.x;
+    const uint32_t* prec = recs + (size_t)pl * nctl * kURec;
+    for (int k = threadIdx.x; k < nctl; k += blockDim.x) pos[__ldg(order + k)] = k;
+    for (int i = threadIdx.x; i < nctl * 17; i += blockDim.x) {
+        const int u = i / 17, f = i - u * 17;
+        const uint32_t* rec = prec + (size_t)u * kURec;
+        const bool ok = rec[kUNT + 18] != 0u;
+        // inadmissible controls share one key that sorts after every other
+        key[i] = ok ? (int32_t)(f < 16 ? rec[kUNT + f] : rec[kUNT + 16]) : 0x7fffffff;
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < nctl; u += blockDim.x) {
+        const int32_t* ku = key + u * 17;
+        int rank = 0;
+        for (int v = 0; v < nctl; ++v) {
+            if (v == u) continue;
+            const int32_t* kv = key + v * 17;
+            int cmp = 0;
+            for (int f = 0; f < 17 && cmp == 0; ++f) cmp = (kv[f] > ku[f]) - (kv[f] < ku[f]);
+            if (cmp < 0 || (cmp == 0 && pos[v] < pos[u])) ++rank;
+        }
+        srt[rank] = u;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nctl; r += blockDim.x) {
+        const int u = srt[r];
+        bool first = r == 0;
+        if (!first) {
+            const int32_t *a = key + u * 17, *b = key + srt[r - 1] * 17;
+            for (int f = 0; f < 17 && !first; ++f) first = a[f] != b[f];
+        }
+        gord[(size_t)pl * nctl + r] = (uint16_t)u | (first ? kGroupFirst : 0u);
+    }
+}
+
+// Shared memory of one k_stencil_r block: two record slots, the plane's
+// group order, two padded window buffers, every control's per-row /
+// per-column successor corners and three slots of the tile's
+// admissibility-mask rows.
+__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2) {
+    return 2 * (size_t)kURec * 4 + (size_t)((nctl + 7) & ~7) * 2 +
+           2 * (size_t)(tile_x + 3) * (n2 + 1) * sizeof(float) +
+           (size_t)nctl * (tile_x + n2) * 2 * sizeof(int32_t) +
+           3 * (size_t)tile_x * mask_words(n2) * sizeof(uint32_t);
+}
+
+// The successor's lower corner and fraction of one tile row (row = true,
+// idx = the row) or one column, rounded as the reference rounds them: x +
+// inc_1 + ... + inc_nsub one add at a time, then (x' - lo) / step, floor
+// (PeregrineSolver.jl:248-279, 399-431).  A row's entry is its window row
+// offset (row - wbase, clamped to the window, times the row stride SB); a
+// column's is the column.  Successors off the table are never admissible;
+// the clamps only keep their (unused) indices inside the window.
+__device__ __forceinline__ int2 succ_entry(const GridT<float>& g, const float* inc, int nsub,
+                                           bool row, int32_t idx, int32_t wbase, int32_t nw,
+                                           int32_t n1, int32_t n2, int32_t SB) {
+    typedef Ar<float> R_;
+    const float x = row ? axisvalue(g, 0, idx) : axisvalue(g, 1, idx);
+    const float lo = row ? g.lo[0] : g.lo[1];
+    const float st = row ? g.step[0] : g.step[1];
+    float xn = x;
+    for (int k = 0; k < nsub; ++k) xn = R_::add(xn, inc[k]);
+    const float f = R_::div(R_::sub(xn, lo), st);
+    const float fl = floorf(f);
+    const float t = R_::sub(f, fl);
+    const float flc = fminf(fmaxf(fl, -2.0f), (float)(row ? n1 + 2 : n2 + 2));
+    const int32_t li = (int32_t)flc;
+    return row ? make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t))
+               : make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
+}
+
+// One work item = (plane, tile of kp.tile_x rows x all columns); block =
+// item.  Needs (tile_x + 3) * n2 <= KR * blockDim.x.  The successor corners
+// of every control depend on the plane, the control and the row or column
+// only: all threads of the block compute them once, at its start.
+template <typename S, bool ARGMIN, int KR>
+__global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
+    k_stencil_r(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
+                const uint32_t* __restrict__ mask, const uint32_t* __restrict__ recs, KParams kp,
+                const uint16_t* __restrict__ gord, double* part_sum, double* part_max,
+                int16_t* argmin) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nctl = kp.nctl;
+    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], W = mask_words(n2);
+    const int32_t TX = kp.tile_x;
+    const int32_t SB = n2 + 1;  // window row stride (one padding column)
+    const int32_t bsz = (TX + 3) * SB;
+    uint32_t* rslot = reinterpret_cast<uint32_t*>(smem_raw);  // [2][kURec]
+    uint16_t* ord = reinterpret_cast<uint16_t*>(rslot + 2 * kURec);
+    float* Bbuf = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));
+    // per control: TX row entries (window offset, x fraction), then n2
+    // column entries (column, y fraction)
+    const int32_t rcs = TX + n2;
+    int2* rcinfo = reinterpret_cast<int2*>(Bbuf + 2 * bsz);
+    uint32_t* mslot = reinterpret_cast<uint32_t*>(rcinfo + nctl * rcs);
+    const int32_t mstride = TX * W;
+    const Layout L = make_layout(kp);
+    GridT<float> g;
+    load_grid(g, kp.g);
+    const float cap = kp.p.cap;
+    const int64_t P = L.P;
+    const int64_t item = blockIdx.x;
+    const int64_t pl = item / kp.tiles_x;
+    const int32_t xt = (int32_t)(item - pl * kp.tiles_x);
+    const int32_t x0 = xt * TX;
+    const int32_t nr = min(TX, n1 - x0);
+    const int32_t ncell = nr * n2;
+    const int32_t nw = nr + 3;  // window rows x0+ox-1 .. x0+ox+nr+1
+    const int32_t nwin = nw * n2;
+    const int T = blockDim.x;
+    const int tid = threadIdx.x;
+    int32_t pq6[4];
+    {
+        int64_t pp = pl;
+        pq6[3] = (int32_t)(pp % L.n[5]); pp /= L.n[5];
+        pq6[2] = (int32_t)(pp % L.n[4]); pp /= L.n[4];
+        pq6[1] = (int32_t)(pp % L.n[3]); pp /= L.n[3];
+        pq6[0] = (int32_t)pp;
+    }
+    const uint32_t* prec = recs + (size_t)pl * nctl * kURec;
+
+    // this thread's tile cells e = tid + q*T: (row a, column j) packed
+    const uint8_t* occ_h = occ + ((int64_t)pq6[0] * n1 + x0) * n2;
+    float best[KR];
+    int bk[ARGMIN ? KR : 1];
+    int32_t caj[KR];  // a << 16 | j
+    uint32_t live = 0;
+#pragma unroll
+    for (int q = 0; q < KR; ++q) {
+        const int32_t e = tid + q * T;
+        best[q] = cap;
+        if constexpr (ARGMIN) bk[q] = 0x7fffffff;
+        const int32_t a = e / n2;
+        caj[q] = (a << 16) | (e - a * n2);
+        if (e < ncell && occ_h[e] == 0) live |= 1u << q;
+    }
+    // this thread's window cells w = tid + k*T: their offset in the padded
+    // window (-1: none); bit k of wlast: cell k is in the last column
+    int32_t wsb[KR];
+    uint32_t wlast = 0;
+#pragma unroll
+    for (int k = 0; k < KR; ++k) {
+        const int32_t w = tid + k * T;
+        const int32_t a = w / n2, j = w - a * n2;
+        wsb[k] = w < nwin ? a * SB + j : -1;
+        if (w < nwin && j == n2 - 1) wlast |= 1u << k;
+    }
+    const uint32_t* mplane = mask + ((size_t)pl * nctl * n1 + x0) * W;
+    const int32_t nmw = nr * W;
+    const int32_t mt = tid >= 32 ? tid - 32 : tid + T - 32;
+    const uint16_t* pg_ord = gord + (size_t)pl * nctl;
+    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(pg_ord + i);
+    __syncthreads();
+    constexpr int kRecVec = kURec / 4;
+    {
+        const int u0 = ord[0] & 0x7fff;
+        if (tid < kRecVec) cp_async16(rslot + 4 * tid, prec + (size_t)u0 * kURec + 4 * tid);
+        for (int32_t k = mt; k < nmw; k += T)
+            cp_async4(mslot + k, mplane + (size_t)u0 * n1 * W + k);
+    }
+    cp_async_commit();
+    {
+        // every control's successor corners, in group order
+        const int32_t per = nr + n2;
+        for (int32_t i = tid; i < nctl * per; i += T) {
+            const int32_t uu = i / per, it = i - uu * per;
+            const uint32_t* rec = prec + (size_t)(ord[uu] & 0x7fff) * kURec;
+            const int4 oi = __ldg(reinterpret_cast<const int4*>(rec + kUNT + 16));
+            if (oi.z == 0) continue;
+            const bool row = it < nr;
+            const float* inc =
+                reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
+            rcinfo[(size_t)uu * rcs + (row ? it : TX + it - nr)] =
+                succ_entry(g, inc, oi.w, row, row ? x0 + it : it - nr, x0 + oi.x - 1, nw, n1, n2,
+                           SB);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    float cv[KR][16];  // the group's corner values of the window cells
+#pragma unroll
+    for (int k = 0; k < KR; ++k)
+#pragma unroll
+        for (int c = 0; c < 16; ++c) cv[k][c] = 0.0f;
+    int32_t wbase = 0;
+    int buf = 0;
+    for (int uu = 0; uu < nctl; ++uu) {
+        const uint32_t ent = ord[uu];
+        const int u = (int)(ent & 0x7fffu);
+        const uint32_t* rec = rslot + (uu & 1) * kURec;
+        const int ms = uu % 3;
+        if (uu + 1 < nctl) {
+            const int un = ord[uu + 1] & 0x7fff;
+            if (tid < kRecVec)
+                cp_async16(rslot + ((uu + 1) & 1) * kURec + 4 * tid,
+                           prec + (size_t)un * kURec + 4 * tid);
+            uint32_t* md = mslot + (ms == 2 ? 0 : ms + 1) * mstride;
+            const uint32_t* msrc = mplane + (size_t)un * n1 * W;
+            for (int32_t k = mt; k < nmw; k += T) cp_async4(md + k, msrc + k);
+        }
+        cp_async_commit();
+        const int4 oi = *reinterpret_cast<const int4*>(rec + kUNT + 16);
+        if (oi.z == 0) {
+            if constexpr (ARGMIN) {
+#pragma unroll
+                for (int q = 0; q < KR; ++q)
+                    if (best[q] == cap && u < bk[q]) bk[q] = u;
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            continue;
+        }
+        const float tau = __uint_as_float(rec[16]);
+        float* B = Bbuf + buf * bsz;
+        const int2* ri = rcinfo + uu * rcs;
+        const int2* ci = ri + TX;
+        buf ^= 1;
+
+        // a new group: its corner values of this thread's window cells
+        if (ent & kGroupFirst) {
+            wbase = x0 + oi.x - 1;
+#pragma unroll
+            for (int k = 0; k < KR; ++k) {
+                if (wsb[k] < 0) continue;
+                const int32_t a = wsb[k] / SB, j = wsb[k] - a * SB;
+                const int32_t r = min(max(wbase + a, 0), n1 - 1);
+                const S* base = Vin + (int64_t)r * n2 + j;
+#pragma unroll
+                for (int c = 0; c < 16; ++c)
+                    cv[k][c] = Conv<S>::ld(base + (int64_t)rec[kUNT + c] * P);
+            }
+        }
+
+        // phase 1a: blend, 16 FMAs per window cell from registers
+        {
+            float acc[KR];
+#pragma unroll
+            for (int k = 0; k < KR; ++k) acc[k] = 0.0f;
+#pragma unroll
+            for (int c4 = 0; c4 < 4; ++c4) {
+                const float4 w = reinterpret_cast<const float4*>(rec)[c4];
+#pragma unroll
+                for (int k = 0; k < KR; ++k) {
+                    acc[k] = fmaf(w.x, cv[k][4 * c4 + 0], acc[k]);
+                    acc[k] = fmaf(w.y, cv[k][4 * c4 + 1], acc[k]);
+                    acc[k] = fmaf(w.z, cv[k][4 * c4 + 2], acc[k]);
+                    acc[k] = fmaf(w.w, cv[k][4 * c4 + 3], acc[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < KR; ++k) {
+                if (wsb[k] < 0) continue;
+                B[wsb[k]] = acc[k];
+                // the padding column repeats the last one
+                if ((wlast >> k) & 1u) B[wsb[k] + 1] = acc[k];
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+
+        // phase 2: shift, admissibility, tau, min
+        const uint32_t* mctl = mslot + ms * mstride;
+#pragma unroll
+        for (int q = 0; q < KR; ++q) {
+            // occupied cells and cells past the tile keep their value
+            if (!((live >> q) & 1u)) continue;
+            const int32_t a = caj[q] >> 16, j = caj[q] & 0xffff;
+            const bool adm = (mctl[a * W + (j >> 5)] >> (j & 31)) & 1u;
+            // computed for every cell (its entries are clamped into the
+            // window), kept where admissible
+            const int2 rr = ri[a];
+            const int2 cc = ci[j];
+            const float tx = __int_as_float(rr.y), ty = __int_as_float(cc.y);
+            const float* p = B + rr.x + cc.x;
+            const float v00 = p[0], v01 = p[1], v10 = p[SB], v11 = p[SB + 1];
+            const float m0 = fmaf(tx, v10 - v00, v00);
+            const float m1 = fmaf(tx, v11 - v01, v01);
+            const float val = fmaf(ty, m1 - m0, m0);
+            const float cvl = adm ? fminf(tau + fminf(val, cap), cap) : cap;
+            if constexpr (ARGMIN) {
+                if (cvl < best[q] || (cvl == best[q] && u < bk[q])) {
+                    best[q] = cvl;
+                    bk[q] = u;
+                }
+            } else {
+                best[q] = fminf(best[q], cvl);
+            }
+        }
+    }
+
+    // write V' and the residual partials
+    const S* Vp0 = Vin + pl * P + (int64_t)x0 * n2;
+    S* Vo0 = Vout + pl * P + (int64_t)x0 * n2;
+    double dsum = 0.0, dmax = 0.0;
+#pragma unroll
+    for (int q = 0; q < KR; ++q) {
+        const int32_t e = tid + q * T;
+        if (e >= ncell) break;
+        const S ov = Vp0[e];
+        const float old = (float)Conv<S>::val(ov);
+        const bool lv = (live >> q) & 1u;
+        if constexpr (ARGMIN)
+            argmin[L.rowmajor(x0 + (caj[q] >> 16), caj[q] & 0xffff, pq6[0], pq6[1], pq6[2],
+                              pq6[3])] = lv ? (int16_t)bk[q] : (int16_t)-1;
+        if (lv && (best[q] < old || (kp.relax && old > 0.0f && best[q] != old))) {
+            const S nv = Conv<S>::template st<float>(best[q]);
+            const float nvT = (float)Conv<S>::val(nv);
+            Vo0[e] = nv;
+            const double d = fabs((double)old - (double)nvT);
+            dsum += d;
+            dmax = fmax(dmax, d);
+        } else {
+            Vo0[e] = ov;
+        }
+    }
+    block_partial_at(dsum, dmax, part_sum, part_max, item);
+}

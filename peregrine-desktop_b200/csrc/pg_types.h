@@ -17,6 +17,9 @@ constexpr int kCellThreads = 128;
 // Blend-then-shift sweep: cells per thread, cells per block at most.
 constexpr int kBCells = 4;
 constexpr int kBMaxTileCells = 1024;
+// register-resident blend: window cells per block, and per thread
+constexpr int kRMaxWindowHost = 2048;
+constexpr int kRCellsPerThread = 4;
 // Model entries the adjoint differentiates (diagonals of B, A, S, D; q; c).
 constexpr int kNThetaHost = 18;
 
@@ -47,6 +50,9 @@ struct KParams {
     int32_t btile_x;  // blend-then-shift: x rows per block (0: not eligible)
     int32_t btiles_x; // blend-then-shift: blocks per plane
     int32_t bblock;   // blend-then-shift: threads per block
+    int32_t rtile_x;  // register-resident blend: x rows per block (0: not eligible)
+    int32_t rtiles_x; // register-resident blend: blocks per plane
+    int32_t rblock;   // register-resident blend: threads per block
     int32_t relax;    // 0: V' = min(V, T V), the reference's update; 1: V' = T V except
                       // where V = 0 (target cells, which stay pinned)
     int32_t phase;

@@ -25,7 +25,7 @@ STORE_Q16 = 4
 STORAGES = {"fp32": STORE_F32, "fp16": STORE_F16, "bf16": STORE_BF16, "fp64": STORE_F64,
             "q16": STORE_Q16}
 (KERNEL_AUTO, KERNEL_STENCIL, KERNEL_CELLFORM, KERNEL_STENCIL_EXACT, KERNEL_STENCIL_ROWS,
- KERNEL_STENCIL_GATHER) = (0, 1, 2, 3, 4, 5)
+ KERNEL_STENCIL_GATHER, KERNEL_STENCIL_BLEND) = (0, 1, 2, 3, 4, 5, 6)
 DTYPE_CODES = {"u8": 0, "u16": 1, "f16": 2, "f32": 3}
 
 # Every symbol include/peregrine_hjb.h declares.

@@ -123,6 +123,36 @@ def test_one_sweep_blend_tiles(og, n, storage):
     assert np.mean(gam[free] == am[free]) >= ARGMIN_AGREE
 
 
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16", "q16"])
+@pytest.mark.parametrize("n,rows,cs", [((40, 48, 8, 5, 5, 5), 0, "cube3"),
+                                       ((36, 44, 8, 5, 5, 5), 0, "cube3"),
+                                       ((24, 96, 4, 5, 5, 5), 0, "cube3"),
+                                       ((40, 48, 8, 5, 5, 5), 5, "cube3"),
+                                       ((17, 20, 8, 5, 5, 5), 0, "cube3"),
+                                       ((24, 48, 8, 7, 7, 7), 0, "cube5")])
+def test_register_blend_matches_blend_bit_for_bit(n, rows, cs, storage):
+    """The register-resident blend (controls of a plane in corner-group
+    order, corner values held in registers) against the re-reading blend:
+    same FMA chain, same successor rounding, so four sweeps give the same
+    stored values, residuals and argmin bit for bit -- on one- and multi-tile
+    planes, the 512-thread window of 96 columns, and an explicit tiling."""
+    pr = Problem("tiny", seed=7, n=n, control_set=cs)
+    V = init_value(pr)
+    out = {}
+    for kern in (_lib.KERNEL_STENCIL, _lib.KERNEL_STENCIL_BLEND):
+        with gpu_ctx(pr, storage) as ctx:
+            if rows:
+                ctx.set_tile_rows(rows)
+            ctx.set_value(V)
+            res = [ctx.sweep(phase=ph, kernel=kern)[:2] for ph in range(4)]
+            _, _, am = ctx.sweep(phase=4, kernel=kern, argmin=True)
+            out[kern] = (ctx.get_value(), res, am)
+    a, b = out[_lib.KERNEL_STENCIL], out[_lib.KERNEL_STENCIL_BLEND]
+    assert np.array_equal(a[0], b[0]), f"max |dV| {np.max(np.abs(a[0] - b[0]))}"
+    assert a[1] == b[1]
+    assert np.array_equal(a[2], b[2])
+
+
 def test_one_sweep_small_slab_bit_exact(og):
     """The 24x24x16x9x9x9 workload (27 controls), one x-slab against the oracle."""
     pr = Problem("small", seed=0)
