@@ -85,7 +85,10 @@ struct pg_ctx {
     bool blend_ok = false;   // the blend-then-shift tiling fits (shared memory, row width)
     bool gather_ok = false;  // the 64-corner masked gather fits its shared memory
     uint16_t* gord_d = nullptr;  // per plane, its controls in corner-group order
-    bool rblend_ok = false;      // the register-resident blend can run (gord_d, tiling)
+    uint32_t* rctab_d = nullptr; // per (plane, control, row / column), successor entries
+    uint32_t* tmask_d = nullptr; // admissibility per (plane, tile, control) in tile order
+    size_t tmask_cap = 0;
+    bool rblend_ok = false;      // the register-resident blend can run (tables, tiling)
     int8_t* pol_d = nullptr;
     double* part_sum = nullptr;
     double* part_max = nullptr;
@@ -123,6 +126,11 @@ struct pg_ctx {
         gather_ok = false;
         if (gord_d) cudaFree(gord_d);
         gord_d = nullptr;
+        if (rctab_d) cudaFree(rctab_d);
+        rctab_d = nullptr;
+        if (tmask_d) cudaFree(tmask_d);
+        tmask_d = nullptr;
+        tmask_cap = 0;
         rblend_ok = false;
         if (pol_d) cudaFree(pol_d);
         if (part_sum) cudaFree(part_sum);
@@ -215,6 +223,36 @@ bool r_smem_fits(const pg::KParams& kp) {
            pg::stencil_r_smem_bytes(kp) <= (size_t)(kp.rblock > 256 ? 200 : 100) * 1024;
 }
 
+// (Re)builds the tile-order mask of the register-resident blend for the
+// current tiling and sets rblend_ok.  The blend stays off (the re-reading
+// blend runs) when its tables or the mask do not fit in device memory with
+// 2 GiB to spare.
+int build_r_tables(pg_ctx* ctx) {
+    pg::KParams& kp = ctx->kp;
+    ctx->rblend_ok = false;
+    if (!ctx->mask_ok || !ctx->gord_d || !ctx->rctab_d || !r_smem_fits(kp)) return PG_OK;
+    const size_t need = pg::stencil_tmask_bytes(kp);
+    if (need > ctx->tmask_cap) {
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (ctx->tmask_d) cudaFree(ctx->tmask_d);
+        ctx->tmask_d = nullptr;
+        ctx->tmask_cap = 0;
+        size_t fr = 0, tot = 0;
+        PG_CUDA(cudaMemGetInfo(&fr, &tot));
+        if (need + ((size_t)2 << 30) > fr || cudaMalloc(&ctx->tmask_d, need) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->tmask_d = nullptr;
+            return PG_OK;
+        }
+        ctx->tmask_cap = need;
+    }
+    cudaError_t e = pg::launch_stencil_tmask(ctx->mask_d, kp, ctx->tmask_d, ctx->stream,
+                                             &ctx->launches);
+    if (e != cudaSuccess) return fail(PG_ECUDA, std::string("tile mask: ") + cudaGetErrorString(e));
+    ctx->rblend_ok = true;
+    return PG_OK;
+}
+
 int pick_kernel(pg_ctx* ctx, int32_t kernel, int* out) {
     if (kernel == PG_KERNEL_AUTO) kernel = ctx->stencil_ok ? PG_KERNEL_STENCIL : PG_KERNEL_CELLFORM;
     if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_EXACT) && !ctx->stencil_ok)
@@ -251,8 +289,8 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
                                 use_pol ? ctx->pol_d : nullptr, ctx->kp, ctx->ctl_d, sb, argmin_d,
                                 ctx->stream, &ctx->launches);
     else if (kernel == PG_KERNEL_STENCIL && r_ok)
-        e = pg::launch_stencil_r(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
-                                 ctx->kp, ctx->gord_d, sb, argmin_d, ctx->stream,
+        e = pg::launch_stencil_r(ctx->storage, vin, vout, ctx->occ_d, ctx->recs_d, ctx->tmask_d,
+                                 ctx->rctab_d, ctx->kp, ctx->gord_d, sb, argmin_d, ctx->stream,
                                  &ctx->launches);
     else if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_BLEND) && b_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
@@ -565,18 +603,30 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
             ctx->mask_ok = true;
             ctx->blend_ok = kp.btile_x > 0 && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
             ctx->gather_ok = pg::stencil_u_smem_bytes(kp) <= 200 * 1024;
-            // the register-resident blend's per-plane control order
+            // the register-resident blend's per-plane control order,
+            // successor entries and tile-order mask
+            size_t fr2 = 0, tot2 = 0;
+            PG_CUDA(cudaMemGetInfo(&fr2, &tot2));
+            const size_t gb = (size_t)kp.nplanes * kp.nctl * sizeof(uint16_t);
+            const size_t rcb = pg::stencil_rc_bytes(kp);
             if (kp.rtile_x > 0 && kp.nctl <= 0x7fff && r_smem_fits(kp) &&
-                cudaMalloc(&ctx->gord_d, (size_t)kp.nplanes * kp.nctl * sizeof(uint16_t)) ==
-                    cudaSuccess) {
+                gb + rcb + pg::stencil_tmask_bytes(kp) + ((size_t)2 << 30) < fr2 &&
+                cudaMalloc(&ctx->gord_d, gb) == cudaSuccess &&
+                cudaMalloc(&ctx->rctab_d, rcb) == cudaSuccess) {
                 e = pg::launch_stencil_group(ctx->recs_d, kp, ctx->order_d, ctx->gord_d,
                                              ctx->stream, &ctx->launches);
+                if (e == cudaSuccess)
+                    e = pg::launch_stencil_rc(ctx->recs_d, kp, ctx->rctab_d, ctx->stream,
+                                              &ctx->launches);
                 if (e != cudaSuccess)
                     return fail(PG_ECUDA, std::string("group: ") + cudaGetErrorString(e));
-                ctx->rblend_ok = true;
+                int rc2 = build_r_tables(ctx);
+                if (rc2) return rc2;
             } else {
                 cudaGetLastError();
+                if (ctx->gord_d) cudaFree(ctx->gord_d);
                 ctx->gord_d = nullptr;
+                ctx->rctab_d = nullptr;
             }
         } else {
             cudaGetLastError();
@@ -887,8 +937,9 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
     const void* vin = ctx->V[ctx->cur];
     void* spare = ctx->V[1 - ctx->cur];
     if (ctx->rblend_ok)
-        e = pg::launch_stencil_r(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
-                                 kp, ctx->gord_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
+        e = pg::launch_stencil_r(ctx->storage, vin, spare, ctx->occ_d, ctx->recs_d, ctx->tmask_d,
+                                 ctx->rctab_d, kp, ctx->gord_d, sb, ctx->argmin_d, ctx->stream,
+                                 &ctx->launches);
     else if (ctx->blend_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  kp, ctx->order_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
@@ -1013,8 +1064,7 @@ int pg_set_tile_rows(pg_ctx* ctx, int32_t rows) {
     }
     ctx->blend_ok = ctx->mask_ok && b_fits && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
     r_tiling(kp, r_fits ? rows : -1);
-    ctx->rblend_ok = ctx->gord_d && kp.rtile_x > 0 && r_smem_fits(kp);
-    return PG_OK;
+    return build_r_tables(ctx);
 }
 
 }  // extern "C"

@@ -1060,9 +1060,9 @@ cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const 
 
 template <typename S, bool ARGMIN, int KR>
 static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
-                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
-                               const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
-                               cudaStream_t st, int64_t* launches) {
+                               const uint32_t* recs, const uint32_t* tmask, const uint32_t* rctab,
+                               const KParams& kp, const uint16_t* gord, const SweepBufs& sb,
+                               int16_t* argmin, cudaStream_t st, int64_t* launches) {
     if (kp.rtile_x <= 0 || kp.rblock <= 0 || kp.rblock > RShape<KR>::kMaxThreads ||
         kp.rblock % 32 != 0 || kp.nsub > kStencilMaxSub || kp.g.n[1] > 0xffff ||
         (int64_t)(kp.rtile_x + 3) * kp.g.n[1] > (int64_t)kp.rblock * KR)
@@ -1083,7 +1083,8 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
         attr_set |= attr_bit;
     }
     k_stencil_r<S, ARGMIN, KR><<<(unsigned)blocks, kp.rblock, smem, st>>>(
-        (const S*)Vin, (S*)Vout, occ, mask, recs, kr, gord, sb.part_sum, sb.part_max, argmin);
+        (const S*)Vin, (S*)Vout, occ, recs, tmask, rctab, kr, gord, sb.part_sum, sb.part_max,
+        argmin);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
@@ -1092,14 +1093,14 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
 }
 
 cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uint8_t* occ,
-                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
-                             const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
-                             cudaStream_t st, int64_t* launches) {
+                             const uint32_t* recs, const uint32_t* tmask, const uint32_t* rctab,
+                             const KParams& kp, const uint16_t* gord, const SweepBufs& sb,
+                             int16_t* argmin, cudaStream_t st, int64_t* launches) {
 #define PG_SR(S)                                                                                 \
-    return argmin ? stencil_r_t<S, true, kRCellsPerThread>(Vin, Vout, occ, mask, recs, kp, gord, \
-                                                           sb, argmin, st, launches)             \
-                  : stencil_r_t<S, false, kRCellsPerThread>(Vin, Vout, occ, mask, recs, kp,      \
-                                                            gord, sb, argmin, st, launches)
+    return argmin ? stencil_r_t<S, true, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rctab,   \
+                                                           kp, gord, sb, argmin, st, launches)   \
+                  : stencil_r_t<S, false, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rctab,  \
+                                                            kp, gord, sb, argmin, st, launches)
     switch (storage) {
         case PG_STORE_F32: PG_SR(float);
         case PG_STORE_F16: PG_SR(__half);
@@ -1108,6 +1109,32 @@ cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uin
     }
 #undef PG_SR
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_stencil_rc(const uint32_t* recs, const KParams& kp, uint32_t* rctab,
+                              cudaStream_t st, int64_t* launches) {
+    const int64_t total = kp.nplanes * kp.nctl * (kp.g.n[0] + kp.g.n[1]);
+    k_stencil_rc<<<grid_for(total, 256), 256, 0, st>>>(recs, kp, rctab);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, uint32_t* tmask,
+                                 cudaStream_t st, int64_t* launches) {
+    if (kp.rtile_x <= 0) return cudaErrorInvalidValue;
+    const int64_t total = stencil_tmask_bytes(kp) / 4;
+    k_stencil_tmask<<<grid_for(total, 256), 256, 0, st>>>(mask, kp, kp.rtile_x, kp.rtiles_x, tmask);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+size_t stencil_rc_bytes(const KParams& kp) {
+    return (size_t)kp.nplanes * kp.nctl * (kp.g.n[0] + kp.g.n[1]) * sizeof(uint32_t);
+}
+
+size_t stencil_tmask_bytes(const KParams& kp) {
+    return (size_t)kp.nplanes * kp.rtiles_x * kp.nctl * tile_mask_words(kp.rtile_x, kp.g.n[1]) *
+           sizeof(uint32_t);
 }
 
 size_t stencil_r_smem_bytes(const KParams& kp) {

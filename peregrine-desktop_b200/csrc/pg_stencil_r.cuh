@@ -14,11 +14,18 @@
 //   (corner planes, x offset) and flags the first control of each group;
 //   controls that no cell of the plane admits go last;
 //
-//   k_stencil_r loads, at the first control of each group, the 16 corner
-//   values of each of its window cells into registers (KR cells per thread),
-//   and for every control of the group blends them with the control's 16
-//   weights -- 16 FMAs per window cell from registers, nothing re-read --
-//   into the shared window, then shifts exactly as k_stencil_b does.
+//   k_stencil_rc (once per solve) stores each (plane, control, row or
+//   column)'s successor corner and fraction, which k_stencil_b recomputes
+//   every sweep, and k_stencil_tmask (once per tiling) regroups the
+//   admissibility mask per (plane, tile, control) in tile order;
+//
+//   k_stencil_r stages a block's per-control data (weights, tau, mask words,
+//   successor entries) in shared memory, loads at the first control of each
+//   group the 16 corner values of each of its window cells into registers
+//   (KR cells per thread), and for every control of the group blends them
+//   with the control's 16 weights -- 16 FMAs per window cell from registers,
+//   nothing re-read -- into the shared window, then shifts exactly as
+//   k_stencil_b does.
 //
 // The arithmetic is k_stencil_b's, operation for operation: the same FMA
 // chain over the corners in record order, the same per-row / per-column
@@ -88,27 +95,15 @@ __global__ void __launch_bounds__(128)
     }
 }
 
-// Shared memory of one k_stencil_r block: two record slots, the plane's
-// group order, two padded window buffers, every control's per-row /
-// per-column successor corners and three slots of the tile's
-// admissibility-mask rows.
-__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2) {
-    return 2 * (size_t)kURec * 4 + (size_t)((nctl + 7) & ~7) * 2 +
-           2 * (size_t)(tile_x + 3) * (n2 + 1) * sizeof(float) +
-           (size_t)nctl * (tile_x + n2) * 2 * sizeof(int32_t) +
-           3 * (size_t)tile_x * mask_words(n2) * sizeof(uint32_t);
-}
-
-// The successor's lower corner and fraction of one tile row (row = true,
+// The successor's lower corner li and fraction t of one row (row = true,
 // idx = the row) or one column, rounded as the reference rounds them: x +
-// inc_1 + ... + inc_nsub one add at a time, then (x' - lo) / step, floor
-// (PeregrineSolver.jl:248-279, 399-431).  A row's entry is its window row
-// offset (row - wbase, clamped to the window, times the row stride SB); a
-// column's is the column.  Successors off the table are never admissible;
-// the clamps only keep their (unused) indices inside the window.
-__device__ __forceinline__ int2 succ_entry(const GridT<float>& g, const float* inc, int nsub,
-                                           bool row, int32_t idx, int32_t wbase, int32_t nw,
-                                           int32_t n1, int32_t n2, int32_t SB) {
+// inc_1 + ... + inc_nsub one add at a time, then (x' - lo) / step and its
+// floor (PeregrineSolver.jl:248-279, 399-431).  li is clamped to
+// [-2, n + 2]: successors off the table are never admissible, and the clamp
+// only keeps their (unused) indices small.
+__device__ __forceinline__ void succ_li_t(const GridT<float>& g, const float* inc, int nsub,
+                                          bool row, int32_t idx, int32_t n1, int32_t n2,
+                                          int32_t* li, float* t) {
     typedef Ar<float> R_;
     const float x = row ? axisvalue(g, 0, idx) : axisvalue(g, 1, idx);
     const float lo = row ? g.lo[0] : g.lo[1];
@@ -117,38 +112,121 @@ __device__ __forceinline__ int2 succ_entry(const GridT<float>& g, const float* i
     for (int k = 0; k < nsub; ++k) xn = R_::add(xn, inc[k]);
     const float f = R_::div(R_::sub(xn, lo), st);
     const float fl = floorf(f);
-    const float t = R_::sub(f, fl);
-    const float flc = fminf(fmaxf(fl, -2.0f), (float)(row ? n1 + 2 : n2 + 2));
-    const int32_t li = (int32_t)flc;
-    return row ? make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t))
-               : make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
+    *t = R_::sub(f, fl);
+    *li = (int32_t)fminf(fmaxf(fl, -2.0f), (float)(row ? n1 + 2 : n2 + 2));
+}
+
+// Packed successor entry of a (plane, control, row or column): the fraction
+// t in bits 0-29 (t is in [0, 1), so its sign and top exponent bit are 0)
+// and d = li - idx - (offset - 1) in bits 30-31, where offset is the
+// control's nominal x (rows) or y (columns) offset; d = 3 marks an entry
+// outside offset - 1 .. offset + 1 (or a t out of range), which the sweep
+// recomputes.
+constexpr uint32_t kRcSlow = 3u << 30;
+
+// Once per solve: the packed entries of every (plane, control), n1 rows
+// then n2 columns.  Inadmissible controls get 0 (never read).
+__global__ void k_stencil_rc(const uint32_t* __restrict__ recs, KParams kp,
+                             uint32_t* __restrict__ rctab) {
+    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], per = n1 + n2;
+    GridT<float> g;
+    load_grid(g, kp.g);
+    const int64_t total = kp.nplanes * kp.nctl * per;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pu = i / per;
+        const int32_t it = (int32_t)(i - pu * per);
+        const uint32_t* rec = recs + (size_t)pu * kURec;
+        if (__ldg(rec + kUNT + 18) == 0u) {
+            rctab[i] = 0u;
+            continue;
+        }
+        const bool row = it < n1;
+        const int32_t idx = row ? it : it - n1;
+        const int32_t off = (int32_t)__ldg(rec + kUNT + (row ? 16 : 17));
+        const float* inc = reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
+        int32_t li;
+        float t;
+        succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
+        const int32_t d = li - idx - off + 1;
+        const uint32_t tb = __float_as_uint(t);
+        rctab[i] = (d >= 0 && d <= 2 && t >= 0.0f && t < 1.0f) ? ((uint32_t)d << 30) | tb : kRcSlow;
+    }
+}
+
+// Words of one tile's admissibility bits in tile order (bit e of the tile =
+// cell e = a * n2 + j of its rows), per control.
+__host__ __device__ inline int32_t tile_mask_words(int32_t tile_x, int32_t n2) {
+    return (tile_x * n2 + 31) / 32;
+}
+
+// Once per tiling: the admissibility mask regrouped per (plane, tile,
+// control) in tile order, from the per-row layout of k_stencil_prep.
+__global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, int32_t tile_x,
+                                int32_t tiles_x, uint32_t* __restrict__ tmask) {
+    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], W = mask_words(n2);
+    const int32_t MW = tile_mask_words(tile_x, n2);
+    const int nctl = kp.nctl;
+    const int64_t total = kp.nplanes * tiles_x * nctl * MW;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = i / MW;
+        const int32_t w = (int32_t)(i - r * MW);
+        const int32_t u = (int32_t)(r % nctl);
+        r /= nctl;
+        const int32_t xt = (int32_t)(r % tiles_x);
+        const int64_t pl = r / tiles_x;
+        const int32_t x0 = xt * tile_x;
+        const int32_t ncell = min(tile_x, n1 - x0) * n2;
+        const uint32_t* mrow = mask + ((size_t)pl * nctl + u) * n1 * W;
+        uint32_t word = 0;
+        int32_t e = 32 * w;
+        int32_t a = e / n2, j = e - a * n2;
+        for (int b = 0; b < 32 && e < ncell; ++b, ++e) {
+            word |= ((__ldg(mrow + (x0 + a) * W + (j >> 5)) >> (j & 31)) & 1u) << b;
+            if (++j == n2) { j = 0; ++a; }
+        }
+        tmask[i] = word;
+    }
+}
+
+// Shared memory of one k_stencil_r block: the plane's group order, per
+// control its 16 weights, tau, admissibility and x offset (20 words), its
+// tile mask words and its successor entries, and two padded window buffers.
+constexpr int kRWt = 20;
+__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2) {
+    return (size_t)((nctl + 7) & ~7) * 2 + (size_t)nctl * kRWt * 4 +
+           (size_t)nctl * tile_mask_words(tile_x, n2) * 4 + 4 +
+           (size_t)nctl * (tile_x + n2) * 2 * sizeof(int32_t) +
+           2 * (size_t)(tile_x + 3) * (n2 + 1) * sizeof(float);
 }
 
 // One work item = (plane, tile of kp.tile_x rows x all columns); block =
-// item.  Needs (tile_x + 3) * n2 <= KR * blockDim.x.  The successor corners
-// of every control depend on the plane, the control and the row or column
-// only: all threads of the block compute them once, at its start.
+// item.  Needs (tile_x + 3) * n2 <= KR * blockDim.x and blockDim.x a
+// multiple of 32.  The block first stages what its controls need into
+// shared memory; the control loop then reads nothing else but the corner
+// values at the start of each group.
 template <typename S, bool ARGMIN, int KR>
 __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
     k_stencil_r(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
-                const uint32_t* __restrict__ mask, const uint32_t* __restrict__ recs, KParams kp,
-                const uint16_t* __restrict__ gord, double* part_sum, double* part_max,
-                int16_t* argmin) {
+                const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
+                const uint32_t* __restrict__ rctab, KParams kp, const uint16_t* __restrict__ gord,
+                double* part_sum, double* part_max, int16_t* argmin) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nctl = kp.nctl;
-    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], W = mask_words(n2);
+    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
     const int32_t TX = kp.tile_x;
     const int32_t SB = n2 + 1;  // window row stride (one padding column)
     const int32_t bsz = (TX + 3) * SB;
-    uint32_t* rslot = reinterpret_cast<uint32_t*>(smem_raw);  // [2][kURec]
-    uint16_t* ord = reinterpret_cast<uint16_t*>(rslot + 2 * kURec);
-    float* Bbuf = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));
-    // per control: TX row entries (window offset, x fraction), then n2
-    // column entries (column, y fraction)
-    const int32_t rcs = TX + n2;
-    int2* rcinfo = reinterpret_cast<int2*>(Bbuf + 2 * bsz);
-    uint32_t* mslot = reinterpret_cast<uint32_t*>(rcinfo + nctl * rcs);
-    const int32_t mstride = TX * W;
+    const int32_t MW = tile_mask_words(TX, n2);
+    const int32_t rcs = TX + n2;  // successor entries per control
+    uint16_t* ord = reinterpret_cast<uint16_t*>(smem_raw);
+    float* wt = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));  // [nctl][kRWt]
+    uint32_t* msk = reinterpret_cast<uint32_t*>(wt + nctl * kRWt);   // [nctl][MW]
+    // [nctl][rcs]: TX rows (window offset, x fraction), n2 columns (column,
+    // y fraction)
+    int2* rcinfo = reinterpret_cast<int2*>(msk + nctl * MW + ((nctl * MW) & 1));
+    float* Bbuf = reinterpret_cast<float*>(rcinfo + nctl * rcs);
     const Layout L = make_layout(kp);
     GridT<float> g;
     load_grid(g, kp.g);
@@ -173,6 +251,48 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         pq6[0] = (int32_t)pp;
     }
     const uint32_t* prec = recs + (size_t)pl * nctl * kURec;
+
+    // stage the block's per-control data
+    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
+    for (int i = tid; i < nctl * kRWt; i += T) {
+        const int u = i / kRWt, f = i - u * kRWt;
+        const uint32_t* rec = prec + (size_t)u * kURec;
+        const uint32_t v = f < 17 ? __ldg(rec + f)
+                                  : (f == 17 ? __ldg(rec + kUNT + 18)
+                                             : (f == 18 ? __ldg(rec + kUNT + 16) : 0u));
+        wt[i] = __uint_as_float(v);
+    }
+    {
+        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * MW;
+        for (int i = tid; i < nctl * MW; i += T) msk[i] = __ldg(src + i);
+    }
+    {
+        const int32_t per = nr + n2;
+        for (int32_t i = tid; i < nctl * per; i += T) {
+            const int32_t u = i / per, it = i - u * per;
+            const bool row = it < nr;
+            const int32_t idx = row ? x0 + it : it - nr;
+            const uint32_t* rec = prec + (size_t)u * kURec;
+            const uint32_t e =
+                __ldg(rctab + ((size_t)pl * nctl + u) * (n1 + n2) + (row ? idx : n1 + idx));
+            const int32_t off = (int32_t)__ldg(rec + kUNT + (row ? 16 : 17));
+            int32_t li;
+            float t;
+            if ((e & kRcSlow) == kRcSlow) {
+                if (__ldg(rec + kUNT + 18) == 0u) continue;  // never read
+                const float* inc =
+                    reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
+                succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
+            } else {
+                li = idx + off - 1 + (int32_t)(e >> 30);
+                t = __uint_as_float(e & ~kRcSlow);
+            }
+            const int32_t wbase = x0 + off - 1;
+            rcinfo[(size_t)u * rcs + (row ? it : TX + it - nr)] =
+                row ? make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t))
+                    : make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
+        }
+    }
 
     // this thread's tile cells e = tid + q*T: (row a, column j) packed
     const uint8_t* occ_h = occ + ((int64_t)pq6[0] * n1 + x0) * n2;
@@ -200,37 +320,9 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         wsb[k] = w < nwin ? a * SB + j : -1;
         if (w < nwin && j == n2 - 1) wlast |= 1u << k;
     }
-    const uint32_t* mplane = mask + ((size_t)pl * nctl * n1 + x0) * W;
-    const int32_t nmw = nr * W;
-    const int32_t mt = tid >= 32 ? tid - 32 : tid + T - 32;
-    const uint16_t* pg_ord = gord + (size_t)pl * nctl;
-    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(pg_ord + i);
-    __syncthreads();
-    constexpr int kRecVec = kURec / 4;
-    {
-        const int u0 = ord[0] & 0x7fff;
-        if (tid < kRecVec) cp_async16(rslot + 4 * tid, prec + (size_t)u0 * kURec + 4 * tid);
-        for (int32_t k = mt; k < nmw; k += T)
-            cp_async4(mslot + k, mplane + (size_t)u0 * n1 * W + k);
-    }
-    cp_async_commit();
-    {
-        // every control's successor corners, in group order
-        const int32_t per = nr + n2;
-        for (int32_t i = tid; i < nctl * per; i += T) {
-            const int32_t uu = i / per, it = i - uu * per;
-            const uint32_t* rec = prec + (size_t)(ord[uu] & 0x7fff) * kURec;
-            const int4 oi = __ldg(reinterpret_cast<const int4*>(rec + kUNT + 16));
-            if (oi.z == 0) continue;
-            const bool row = it < nr;
-            const float* inc =
-                reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
-            rcinfo[(size_t)uu * rcs + (row ? it : TX + it - nr)] =
-                succ_entry(g, inc, oi.w, row, row ? x0 + it : it - nr, x0 + oi.x - 1, nw, n1, n2,
-                           SB);
-        }
-    }
-    cp_async_wait_all();
+    // mask word of cell q in a control's tile words; its bit is the lane
+    const int32_t mw0 = tid >> 5, mwq = T >> 5;
+    const uint32_t lane = (uint32_t)tid & 31u;
     __syncthreads();
 
     float cv[KR][16];  // the group's corner values of the window cells
@@ -238,43 +330,27 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
     for (int k = 0; k < KR; ++k)
 #pragma unroll
         for (int c = 0; c < 16; ++c) cv[k][c] = 0.0f;
-    int32_t wbase = 0;
     int buf = 0;
     for (int uu = 0; uu < nctl; ++uu) {
         const uint32_t ent = ord[uu];
         const int u = (int)(ent & 0x7fffu);
-        const uint32_t* rec = rslot + (uu & 1) * kURec;
-        const int ms = uu % 3;
-        if (uu + 1 < nctl) {
-            const int un = ord[uu + 1] & 0x7fff;
-            if (tid < kRecVec)
-                cp_async16(rslot + ((uu + 1) & 1) * kURec + 4 * tid,
-                           prec + (size_t)un * kURec + 4 * tid);
-            uint32_t* md = mslot + (ms == 2 ? 0 : ms + 1) * mstride;
-            const uint32_t* msrc = mplane + (size_t)un * n1 * W;
-            for (int32_t k = mt; k < nmw; k += T) cp_async4(md + k, msrc + k);
-        }
-        cp_async_commit();
-        const int4 oi = *reinterpret_cast<const int4*>(rec + kUNT + 16);
-        if (oi.z == 0) {
+        const float* wu = wt + u * kRWt;
+        if (__float_as_uint(wu[17]) == 0u) {
+            // no cell of the plane admits this control (block-uniform)
             if constexpr (ARGMIN) {
 #pragma unroll
                 for (int q = 0; q < KR; ++q)
                     if (best[q] == cap && u < bk[q]) bk[q] = u;
             }
-            cp_async_wait_all();
-            __syncthreads();
             continue;
         }
-        const float tau = __uint_as_float(rec[16]);
         float* B = Bbuf + buf * bsz;
-        const int2* ri = rcinfo + uu * rcs;
-        const int2* ci = ri + TX;
         buf ^= 1;
 
         // a new group: its corner values of this thread's window cells
         if (ent & kGroupFirst) {
-            wbase = x0 + oi.x - 1;
+            const int32_t wbase = x0 + __float_as_int(wu[18]) - 1;
+            const uint32_t* rec = prec + (size_t)u * kURec;
 #pragma unroll
             for (int k = 0; k < KR; ++k) {
                 if (wsb[k] < 0) continue;
@@ -283,18 +359,18 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
                 const S* base = Vin + (int64_t)r * n2 + j;
 #pragma unroll
                 for (int c = 0; c < 16; ++c)
-                    cv[k][c] = Conv<S>::ld(base + (int64_t)rec[kUNT + c] * P);
+                    cv[k][c] = Conv<S>::ld(base + (int64_t)__ldg(rec + kUNT + c) * P);
             }
         }
 
-        // phase 1a: blend, 16 FMAs per window cell from registers
+        // phase 1: blend, 16 FMAs per window cell from registers
         {
             float acc[KR];
 #pragma unroll
             for (int k = 0; k < KR; ++k) acc[k] = 0.0f;
 #pragma unroll
             for (int c4 = 0; c4 < 4; ++c4) {
-                const float4 w = reinterpret_cast<const float4*>(rec)[c4];
+                const float4 w = reinterpret_cast<const float4*>(wu)[c4];
 #pragma unroll
                 for (int k = 0; k < KR; ++k) {
                     acc[k] = fmaf(w.x, cv[k][4 * c4 + 0], acc[k]);
@@ -311,17 +387,19 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
                 if ((wlast >> k) & 1u) B[wsb[k] + 1] = acc[k];
             }
         }
-        cp_async_wait_all();
         __syncthreads();
 
         // phase 2: shift, admissibility, tau, min
-        const uint32_t* mctl = mslot + ms * mstride;
+        const float tau = wu[16];
+        const int2* ri = rcinfo + u * rcs;
+        const int2* ci = ri + TX;
+        const uint32_t* mu = msk + u * MW + mw0;
 #pragma unroll
         for (int q = 0; q < KR; ++q) {
             // occupied cells and cells past the tile keep their value
             if (!((live >> q) & 1u)) continue;
             const int32_t a = caj[q] >> 16, j = caj[q] & 0xffff;
-            const bool adm = (mctl[a * W + (j >> 5)] >> (j & 31)) & 1u;
+            const bool adm = (mu[q * mwq] >> lane) & 1u;
             // computed for every cell (its entries are clamped into the
             // window), kept where admissible
             const int2 rr = ri[a];
@@ -334,6 +412,8 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
             const float val = fmaf(ty, m1 - m0, m0);
             const float cvl = adm ? fminf(tau + fminf(val, cap), cap) : cap;
             if constexpr (ARGMIN) {
+                // equal values go to the lower table index, which is what
+                // the reference's strict < in table order keeps
                 if (cvl < best[q] || (cvl == best[q] && u < bk[q])) {
                     best[q] = cvl;
                     bk[q] = u;
