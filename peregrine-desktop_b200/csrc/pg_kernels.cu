@@ -1072,7 +1072,7 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
     kr.tiles_x = kp.rtiles_x;
     const int64_t blocks = kp.nplanes * kp.rtiles_x;
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-    const size_t smem = stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1]);
+    const size_t smem = stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, KR);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static uint64_t attr_set = 0;
     const uint64_t attr_bit = device_bit();
@@ -1138,7 +1138,7 @@ size_t stencil_tmask_bytes(const KParams& kp) {
 }
 
 size_t stencil_r_smem_bytes(const KParams& kp) {
-    return stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1]);
+    return stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, kRCellsPerThread);
 }
 
 size_t stencil_b_smem_bytes(const KParams& kp) {

@@ -190,15 +190,23 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
     }
 }
 
-// Shared memory of one k_stencil_r block: the plane's group order, per
-// control its 16 weights, tau, admissibility and x offset (20 words), its
-// tile mask words and its successor entries, and two padded window buffers.
+// Shared memory of one k_stencil_r block of `threads` threads (a multiple of
+// 32) with KR cells per thread: the plane's group order; per control its 16
+// weights, tau, admissibility and x / y offsets (20 words), its mask words
+// (one per warp and cell slot: the tile's words, zero beyond them) and its
+// successor entries; and two padded window buffers with room for every
+// thread's KR window slots (slots past the window land in scratch rows).
 constexpr int kRWt = 20;
-__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2) {
+__host__ __device__ inline int32_t stencil_r_window_rows(int tile_x, int n2, int threads, int kr) {
+    const int32_t slots = (kr * threads + n2 - 1) / n2;
+    return slots > tile_x + 3 ? slots : tile_x + 3;
+}
+__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2, int threads,
+                                                 int kr) {
     return (size_t)((nctl + 7) & ~7) * 2 + (size_t)nctl * kRWt * 4 +
-           (size_t)nctl * tile_mask_words(tile_x, n2) * 4 + 4 +
+           (size_t)nctl * kr * (threads / 32) * 4 + 4 +
            (size_t)nctl * (tile_x + n2) * 2 * sizeof(int32_t) +
-           2 * (size_t)(tile_x + 3) * (n2 + 1) * sizeof(float);
+           2 * (size_t)stencil_r_window_rows(tile_x, n2, threads, kr) * (n2 + 1) * sizeof(float);
 }
 
 // One work item = (plane, tile of kp.tile_x rows x all columns); block =
@@ -216,16 +224,20 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
     const int nctl = kp.nctl;
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
     const int32_t TX = kp.tile_x;
+    const int T = blockDim.x;
+    const int tid = threadIdx.x;
     const int32_t SB = n2 + 1;  // window row stride (one padding column)
-    const int32_t bsz = (TX + 3) * SB;
+    const int32_t bsz = stencil_r_window_rows(TX, n2, T, KR) * SB;
     const int32_t MW = tile_mask_words(TX, n2);
+    const int32_t mwq = T >> 5;          // mask words per cell slot
+    const int32_t MWS = KR * mwq;        // mask words per control in shared memory
     const int32_t rcs = TX + n2;  // successor entries per control
     uint16_t* ord = reinterpret_cast<uint16_t*>(smem_raw);
     float* wt = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));  // [nctl][kRWt]
-    uint32_t* msk = reinterpret_cast<uint32_t*>(wt + nctl * kRWt);   // [nctl][MW]
+    uint32_t* msk = reinterpret_cast<uint32_t*>(wt + nctl * kRWt);   // [nctl][MWS]
     // [nctl][rcs]: TX rows (window offset, x fraction), n2 columns (column,
     // y fraction)
-    int2* rcinfo = reinterpret_cast<int2*>(msk + nctl * MW + ((nctl * MW) & 1));
+    int2* rcinfo = reinterpret_cast<int2*>(msk + nctl * MWS + ((nctl * MWS) & 1));
     float* Bbuf = reinterpret_cast<float*>(rcinfo + nctl * rcs);
     const Layout L = make_layout(kp);
     GridT<float> g;
@@ -239,9 +251,6 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
     const int32_t nr = min(TX, n1 - x0);
     const int32_t ncell = nr * n2;
     const int32_t nw = nr + 3;  // window rows x0+ox-1 .. x0+ox+nr+1
-    const int32_t nwin = nw * n2;
-    const int T = blockDim.x;
-    const int tid = threadIdx.x;
     int32_t pq6[4];
     {
         int64_t pp = pl;
@@ -257,29 +266,33 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
     for (int i = tid; i < nctl * kRWt; i += T) {
         const int u = i / kRWt, f = i - u * kRWt;
         const uint32_t* rec = prec + (size_t)u * kURec;
-        const uint32_t v = f < 17 ? __ldg(rec + f)
-                                  : (f == 17 ? __ldg(rec + kUNT + 18)
-                                             : (f == 18 ? __ldg(rec + kUNT + 16) : 0u));
+        // w[16], tau, ok, ox, oy
+        const int sf = f < 17 ? f : (f == 17 ? kUNT + 18 : (f == 18 ? kUNT + 16 : kUNT + 17));
+        const uint32_t v = __ldg(rec + sf);
         wt[i] = __uint_as_float(v);
     }
     {
         const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * MW;
-        for (int i = tid; i < nctl * MW; i += T) msk[i] = __ldg(src + i);
+        for (int i = tid; i < nctl * MWS; i += T) {
+            const int u = i / MWS, w = i - u * MWS;
+            msk[i] = w < MW ? __ldg(src + (size_t)u * MW + w) : 0u;
+        }
     }
+    __syncthreads();  // wt
     {
         const int32_t per = nr + n2;
         for (int32_t i = tid; i < nctl * per; i += T) {
             const int32_t u = i / per, it = i - u * per;
+            if (__float_as_uint(wt[u * kRWt + 17]) == 0u) continue;  // never read
             const bool row = it < nr;
             const int32_t idx = row ? x0 + it : it - nr;
-            const uint32_t* rec = prec + (size_t)u * kURec;
             const uint32_t e =
                 __ldg(rctab + ((size_t)pl * nctl + u) * (n1 + n2) + (row ? idx : n1 + idx));
-            const int32_t off = (int32_t)__ldg(rec + kUNT + (row ? 16 : 17));
+            const int32_t off = __float_as_int(wt[u * kRWt + (row ? 18 : 19)]);
             int32_t li;
             float t;
             if ((e & kRcSlow) == kRcSlow) {
-                if (__ldg(rec + kUNT + 18) == 0u) continue;  // never read
+                const uint32_t* rec = prec + (size_t)u * kURec;
                 const float* inc =
                     reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
                 succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
@@ -305,31 +318,48 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         const int32_t e = tid + q * T;
         best[q] = cap;
         if constexpr (ARGMIN) bk[q] = 0x7fffffff;
-        const int32_t a = e / n2;
-        caj[q] = (a << 16) | (e - a * n2);
+        // slots past the tile read cell (0, 0) and are never kept
+        const int32_t a = e < ncell ? e / n2 : 0;
+        caj[q] = e < ncell ? (a << 16) | (e - a * n2) : 0;
         if (e < ncell && occ_h[e] == 0) live |= 1u << q;
     }
-    // this thread's window cells w = tid + k*T: their offset in the padded
-    // window (-1: none); bit k of wlast: cell k is in the last column
+    // this thread's window slots w = tid + k*T: their offset in the padded
+    // window (slots past the window fall in its scratch rows); bit k of
+    // wlast: slot k is in the last column
     int32_t wsb[KR];
     uint32_t wlast = 0;
 #pragma unroll
     for (int k = 0; k < KR; ++k) {
         const int32_t w = tid + k * T;
         const int32_t a = w / n2, j = w - a * n2;
-        wsb[k] = w < nwin ? a * SB + j : -1;
-        if (w < nwin && j == n2 - 1) wlast |= 1u << k;
+        wsb[k] = a * SB + j;
+        if (j == n2 - 1) wlast |= 1u << k;
     }
-    // mask word of cell q in a control's tile words; its bit is the lane
-    const int32_t mw0 = tid >> 5, mwq = T >> 5;
+    // mask word of cell slot q in a control's words; its bit is the lane
+    const int32_t mw0 = tid >> 5;
     const uint32_t lane = (uint32_t)tid & 31u;
     __syncthreads();
 
-    float cv[KR][16];  // the group's corner values of the window cells
+    float cv[KR][16];  // the group's corner values of the window slots
+    // corner values of the group that control uu starts: the planes of its
+    // record, rows from its x offset
+    auto load_group = [&](int uu) {
+        const int u = ord[uu] & 0x7fff;
+        const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 18]) - 1;
+        const uint32_t* rec = prec + (size_t)u * kURec;
 #pragma unroll
-    for (int k = 0; k < KR; ++k)
+        for (int k = 0; k < KR; ++k) {
+            const int32_t a = wsb[k] / SB, j = wsb[k] - a * SB;
+            const int32_t r = min(max(wbase + a, 0), n1 - 1);
+            const S* base = Vin + (int64_t)r * n2 + j;
 #pragma unroll
-        for (int c = 0; c < 16; ++c) cv[k][c] = 0.0f;
+            for (int c = 0; c < 16; ++c)
+                cv[k][c] = Conv<S>::ld(base + (int64_t)__ldg(rec + kUNT + c) * P);
+        }
+    };
+    // the first control starts a group; inadmissible controls come last and
+    // their records' corner planes are never read
+    if (__float_as_uint(wt[(ord[0] & 0x7fff) * kRWt + 17]) != 0u) load_group(0);
     int buf = 0;
     for (int uu = 0; uu < nctl; ++uu) {
         const uint32_t ent = ord[uu];
@@ -347,23 +377,7 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         float* B = Bbuf + buf * bsz;
         buf ^= 1;
 
-        // a new group: its corner values of this thread's window cells
-        if (ent & kGroupFirst) {
-            const int32_t wbase = x0 + __float_as_int(wu[18]) - 1;
-            const uint32_t* rec = prec + (size_t)u * kURec;
-#pragma unroll
-            for (int k = 0; k < KR; ++k) {
-                if (wsb[k] < 0) continue;
-                const int32_t a = wsb[k] / SB, j = wsb[k] - a * SB;
-                const int32_t r = min(max(wbase + a, 0), n1 - 1);
-                const S* base = Vin + (int64_t)r * n2 + j;
-#pragma unroll
-                for (int c = 0; c < 16; ++c)
-                    cv[k][c] = Conv<S>::ld(base + (int64_t)__ldg(rec + kUNT + c) * P);
-            }
-        }
-
-        // phase 1: blend, 16 FMAs per window cell from registers
+        // phase 1: blend, 16 FMAs per window slot from registers
         {
             float acc[KR];
 #pragma unroll
@@ -381,27 +395,29 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
             }
 #pragma unroll
             for (int k = 0; k < KR; ++k) {
-                if (wsb[k] < 0) continue;
                 B[wsb[k]] = acc[k];
                 // the padding column repeats the last one
                 if ((wlast >> k) & 1u) B[wsb[k] + 1] = acc[k];
             }
         }
+        // the corner values are free now: if the next control starts a new
+        // group, its loads fly during this control's barrier and phase 2
+        if (uu + 1 < nctl && (ord[uu + 1] & kGroupFirst) &&
+            __float_as_uint(wt[(ord[uu + 1] & 0x7fff) * kRWt + 17]) != 0u)
+            load_group(uu + 1);
         __syncthreads();
 
-        // phase 2: shift, admissibility, tau, min
+        // phase 2: shift, admissibility, tau, min -- computed for every cell
+        // slot (entries are clamped into the window, dead slots read cell
+        // (0, 0)), kept where the cell is free and the control admissible
         const float tau = wu[16];
         const int2* ri = rcinfo + u * rcs;
         const int2* ci = ri + TX;
-        const uint32_t* mu = msk + u * MW + mw0;
+        const uint32_t* mu = msk + u * MWS + mw0;
 #pragma unroll
         for (int q = 0; q < KR; ++q) {
-            // occupied cells and cells past the tile keep their value
-            if (!((live >> q) & 1u)) continue;
             const int32_t a = caj[q] >> 16, j = caj[q] & 0xffff;
-            const bool adm = (mu[q * mwq] >> lane) & 1u;
-            // computed for every cell (its entries are clamped into the
-            // window), kept where admissible
+            const bool adm = ((live >> q) & (mu[q * mwq] >> lane)) & 1u;
             const int2 rr = ri[a];
             const int2 cc = ci[j];
             const float tx = __int_as_float(rr.y), ty = __int_as_float(cc.y);
