@@ -33,6 +33,22 @@
 // bit-identical to it.  The window has one padding column (a copy of the
 // last column), so the upper column corner needs no clamp.
 
+// Two FP32 lanes in one 64-bit register, and the packed FMA of sm_100
+// (fma.rn.f32x2: an IEEE fma per lane, the same result as two fmaf).
+__device__ __forceinline__ uint64_t pk2(float a, float b) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk2(uint64_t v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
 // Controls of a plane in group order: entry = control | kGroupFirst on the
 // first control of a group.
 constexpr uint16_t kGroupFirst = 0x8000u;
@@ -340,21 +356,27 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
     const uint32_t lane = (uint32_t)tid & 31u;
     __syncthreads();
 
-    float cv[KR][16];  // the group's corner values of the window slots
+    static_assert(KR % 2 == 0, "window slots are paired for the packed FMA");
+    uint64_t cv[KR / 2][16];  // the group's corner values, slots 2i and 2i+1 paired
     // corner values of the group that control uu starts: the planes of its
     // record, rows from its x offset
     auto load_group = [&](int uu) {
         const int u = ord[uu] & 0x7fff;
         const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 18]) - 1;
         const uint32_t* rec = prec + (size_t)u * kURec;
+        const S* base[KR];
 #pragma unroll
         for (int k = 0; k < KR; ++k) {
             const int32_t a = wsb[k] / SB, j = wsb[k] - a * SB;
             const int32_t r = min(max(wbase + a, 0), n1 - 1);
-            const S* base = Vin + (int64_t)r * n2 + j;
+            base[k] = Vin + (int64_t)r * n2 + j;
+        }
 #pragma unroll
-            for (int c = 0; c < 16; ++c)
-                cv[k][c] = Conv<S>::ld(base + (int64_t)__ldg(rec + kUNT + c) * P);
+        for (int c = 0; c < 16; ++c) {
+            const int64_t off = (int64_t)__ldg(rec + kUNT + c) * P;
+#pragma unroll
+            for (int k = 0; k < KR; k += 2)
+                cv[k / 2][c] = pk2(Conv<S>::ld(base[k] + off), Conv<S>::ld(base[k + 1] + off));
         }
     };
     // the first control starts a group; inadmissible controls come last and
@@ -379,20 +401,25 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
 
         // phase 1: blend, 16 FMAs per window slot from registers
         {
-            float acc[KR];
+            uint64_t acc2[KR / 2];
 #pragma unroll
-            for (int k = 0; k < KR; ++k) acc[k] = 0.0f;
+            for (int k = 0; k < KR / 2; ++k) acc2[k] = 0ull;
 #pragma unroll
             for (int c4 = 0; c4 < 4; ++c4) {
                 const float4 w = reinterpret_cast<const float4*>(wu)[c4];
+                const uint64_t wx = pk2(w.x, w.x), wy = pk2(w.y, w.y), wz = pk2(w.z, w.z),
+                               ww = pk2(w.w, w.w);
 #pragma unroll
-                for (int k = 0; k < KR; ++k) {
-                    acc[k] = fmaf(w.x, cv[k][4 * c4 + 0], acc[k]);
-                    acc[k] = fmaf(w.y, cv[k][4 * c4 + 1], acc[k]);
-                    acc[k] = fmaf(w.z, cv[k][4 * c4 + 2], acc[k]);
-                    acc[k] = fmaf(w.w, cv[k][4 * c4 + 3], acc[k]);
+                for (int k = 0; k < KR / 2; ++k) {
+                    acc2[k] = fma2(wx, cv[k][4 * c4 + 0], acc2[k]);
+                    acc2[k] = fma2(wy, cv[k][4 * c4 + 1], acc2[k]);
+                    acc2[k] = fma2(wz, cv[k][4 * c4 + 2], acc2[k]);
+                    acc2[k] = fma2(ww, cv[k][4 * c4 + 3], acc2[k]);
                 }
             }
+            float acc[KR];
+#pragma unroll
+            for (int k = 0; k < KR / 2; ++k) upk2(acc2[k], acc[2 * k], acc[2 * k + 1]);
 #pragma unroll
             for (int k = 0; k < KR; ++k) {
                 B[wsb[k]] = acc[k];
