@@ -35,7 +35,7 @@ for _p in (ROOT, PKG):
 METRIC = "Bellman cell-control updates/s; time-to-converge vs plain FP32 at ≤2 ms max err"
 UNIT = "cell-control updates/s"
 WORKLOAD = "medium"
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_stencil_b_medium_fp32.md")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_stencil_r_medium_fp32.md")
 
 
 def peaks():
@@ -47,29 +47,35 @@ def peaks():
 
 
 def blend_tile_rows(n1: int, n2: int) -> int:
-    """Rows per block of the blend-then-shift sweep (the library's tiling:
-    whole rows, at most 1024 cells, as few tiles per plane as that allows)."""
-    tx = min(n1, 1024 // n2)
+    """Rows per block of the register-resident sweep (the library's tiling:
+    whole rows whose window of rows + 3 fits 1024 cells when the 3 extra rows
+    cost at most a quarter, else 2048 cells, balanced over the plane)."""
+    t1 = min(n1, 1024 // n2 - 3)
+    t2 = min(n1, 2048 // n2 - 3)
+    tx = t1 if t1 >= 1 and (t1 == n1 or 4 * (t1 + 3) <= 5 * t1) else t2
     nt = -(-n1 // tx)
     return -(-n1 // nt)
 
 
 def onchip_rooflines(pr, rate_per_gpu: float, elem: int, peaks_onchip) -> dict:
-    """The sweep's on-chip ceilings.  Per cell-control the blend-then-shift
-    kernel reads 16 corner-plane elements per window value ((TX+3)/TX window
-    values per cell) through L1, writes the window to shared memory as FP32
-    and reads 4 of its values back; it spends 16 (TX+3)/TX + 3 FMAs plus an
-    add and two mins."""
+    """The sweep's on-chip ceilings.  Per cell-control the register-resident
+    kernel blends 16 corner values held in registers into (TX+3)/TX window
+    values, writes them to shared memory as FP32 and reads back 4 of them,
+    the row and column successor entries (8 B each) and the mask word (a
+    warp-wide broadcast); it spends 16 (TX+3)/TX + 3 FMAs plus three subtracts
+    and an add.  (The corner planes are read from L2 once per group of
+    controls, not per control.)"""
     n1, n2 = int(pr.grid.n[0]), int(pr.grid.n[1])
     tx = blend_tile_rows(n1, n2)
     win = (tx + 3) / tx
-    bytes_cc = 16 * elem * win + 4 * win + 16
-    flops_cc = 2 * (16 * win + 3) + 3
+    del elem  # the storage type only changes the once-per-group loads
+    bytes_cc = 4 * win + 16 + 8 + 8 + 4 / 32
+    flops_cc = 2 * (16 * win + 3) + 4
     out = {"tile_rows": tx, "bytes_per_update": bytes_cc, "flops_per_update": flops_cc}
     if peaks_onchip:
         g = rate_per_gpu * bytes_cc / 1e9
         f = rate_per_gpu * flops_cc / 1e12
-        out["gather"] = {"achieved": g, "peak": peaks_onchip["smem_gbs"], "unit": "GB/s",
+        out["shared_memory"] = {"achieved": g, "peak": peaks_onchip["smem_gbs"], "unit": "GB/s",
                          "frac": g / peaks_onchip["smem_gbs"],
                          "peak_source": "measured on this GPU (pg_measure_peaks, shared-memory "
                                         "read bandwidth)"}
@@ -200,7 +206,7 @@ def workload_config(pr, extra=None):
         "controls": pr.nctl,
         "step": "one Jacobi sweep over every cell and control",
         "l2": "inputs larger than L2 (V is 0.995 GB per buffer, two buffers)",
-        "kernel": "k_stencil_b<float> (blend-then-shift)",
+        "kernel": "k_stencil_r<float> (register-resident blend-then-shift)",
     }
     if extra:
         cfg.update(extra)
