@@ -1120,15 +1120,29 @@ struct BatchGroup {
     bool off32;  // every table of the group has fewer than 2^32 cells
 };
 
+// The batch runs the register-resident item when every table can (its
+// tables and tile-order mask are built), else the re-reading blend item.
+bool batch_uses_r(const pg_batch* b) {
+    for (const pg_ctx* c : b->tabs)
+        if (!c->rblend_ok) return false;
+    return !b->tabs.empty();
+}
+
 int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, std::vector<int>& perm,
                       std::vector<BatchGroup>& groups, int64_t* nitems, size_t* smem_out) {
     d.clear();
     groups.clear();
     const int ntab = (int)b->tabs.size();
+    const bool use_r = batch_uses_r(b);
+    for (const pg_ctx* c : b->tabs)
+        if (!use_r && !c->blend_ok)
+            return fail(PG_EUNSUPPORTED, "the batch's tables cannot share one blend-then-shift "
+                                         "sweep (mixed eligibility of the two kernels)");
+    auto threads_of = [&](const pg_ctx* c) { return use_r ? c->kp.rblock : c->kp.bblock; };
     perm.resize(ntab);
     for (int t = 0; t < ntab; ++t) perm[t] = t;
     std::stable_sort(perm.begin(), perm.end(), [&](int a, int c) {
-        return b->tabs[a]->kp.bblock < b->tabs[c]->kp.bblock;
+        return threads_of(b->tabs[a]) < threads_of(b->tabs[c]);
     });
     int64_t item = 0;
     size_t smem = 0;
@@ -1142,19 +1156,23 @@ int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, std::
         t.mask = c->mask_d;
         t.recs = c->recs_d;
         t.order = c->order_d;
+        t.tmask = c->tmask_d;
+        t.rctab = c->rctab_d;
+        t.gord = c->gord_d;
         t.kp = c->kp;
-        t.kp.tile_x = c->kp.btile_x;
-        t.kp.tiles_x = c->kp.btiles_x;
+        t.kp.tile_x = use_r ? c->kp.rtile_x : c->kp.btile_x;
+        t.kp.tiles_x = use_r ? c->kp.rtiles_x : c->kp.btiles_x;
         t.item0 = item;
-        t.nitems = c->kp.nplanes * c->kp.btiles_x;
+        t.nitems = c->kp.nplanes * t.kp.tiles_x;
         t.vec = c->kp.g.n[1] % vn == 0 ? 1 : 0;
-        if (groups.empty() || groups.back().threads != c->kp.bblock)
-            groups.push_back(BatchGroup{item, 0, c->kp.bblock, false, false, true});
+        if (groups.empty() || groups.back().threads != threads_of(c))
+            groups.push_back(BatchGroup{item, 0, threads_of(c), false, false, true});
         groups.back().count += t.nitems;
         if (c->kp.ncells > (int64_t)0xffffffffLL) groups.back().off32 = false;
         (t.vec ? groups.back().any_vec : groups.back().any_scalar) = true;
         item += t.nitems;
-        smem = std::max(smem, pg::stencil_b_smem_bytes(c->kp));
+        smem = std::max(smem, use_r ? pg::stencil_r_smem_bytes(c->kp)
+                                    : pg::stencil_b_smem_bytes(c->kp));
         d.push_back(t);
     }
     *nitems = item;
@@ -1171,7 +1189,8 @@ int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_gr
     std::vector<BatchGroup> groups;
     int64_t nitems = 0;
     size_t smem = 0;
-    batch_descriptors(b, st, d, perm, groups, &nitems, &smem);
+    int drc = batch_descriptors(b, st, d, perm, groups, &nitems, &smem);
+    if (drc) return drc;
     const int ntab = (int)b->tabs.size();
     if (nitems > b->cap_items || ntab > b->cap_tabs) {
         b->free_bufs();
@@ -1192,9 +1211,11 @@ int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_gr
                             b->stream));
     int sms = 0;
     PG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    const bool use_r = batch_uses_r(b);
     std::vector<int> grids;
     for (const BatchGroup& gr : groups) {
-        const int per_sm = pg::batch_blocks_per_sm(st, smem, gr.threads);
+        const int per_sm = use_r ? pg::r_batch_blocks_per_sm(st, smem, gr.threads)
+                                 : pg::batch_blocks_per_sm(st, smem, gr.threads);
         if (per_sm <= 0) return fail(PG_EUNSUPPORTED, "the batched sweep does not fit on an SM");
         grids.push_back((int)std::min<int64_t>(gr.count, (int64_t)sms * per_sm));
     }
@@ -1203,11 +1224,15 @@ int batch_phase(pg_batch* b, int st, int32_t max_sweeps, double tol, bool use_gr
         cudaError_t e = cudaSuccess;
         for (int parity = 0; parity < 2 && e == cudaSuccess; ++parity) {
             for (size_t g = 0; g < groups.size() && e == cudaSuccess; ++g)
-                e = pg::launch_stencil_b_batch(st, b->tabs_d, ntab, groups[g].first,
-                                               groups[g].count, groups[g].threads, parity,
-                                               b->done_d, b->part_sum, b->part_max, smem, grids[g],
-                                               groups[g].any_vec, groups[g].any_scalar,
-                                               groups[g].off32, s);
+                e = use_r ? pg::launch_stencil_r_batch(st, b->tabs_d, ntab, groups[g].first,
+                                                       groups[g].count, groups[g].threads, parity,
+                                                       b->done_d, b->part_sum, b->part_max, smem,
+                                                       grids[g], s)
+                          : pg::launch_stencil_b_batch(st, b->tabs_d, ntab, groups[g].first,
+                                                       groups[g].count, groups[g].threads, parity,
+                                                       b->done_d, b->part_sum, b->part_max, smem,
+                                                       grids[g], groups[g].any_vec,
+                                                       groups[g].any_scalar, groups[g].off32, s);
             if (e == cudaSuccess)
                 e = pg::launch_reduce_batch(b->tabs_d, ntab, b->part_sum, b->part_max, b->out_d, s);
         }
@@ -1314,11 +1339,11 @@ int pg_batch_add(pg_batch* b, const pg_grid6* g, const pg_model* m, const pg_par
     int rc = pg_create(&c, b->device);
     if (rc) return rc;
     rc = pg_load_problem(c, g, m, p, occ, ctl, nctl, b->storage);
-    if (!rc && !(c->stencil_ok && c->mask_ok && c->blend_ok))
-        rc = fail(PG_EUNSUPPORTED, "a batched table must run the blend-then-shift sweep (" +
+    if (!rc && tile_rows > 0) rc = pg_set_tile_rows(c, tile_rows);
+    if (!rc && !(c->stencil_ok && c->mask_ok && (c->blend_ok || c->rblend_ok)))
+        rc = fail(PG_EUNSUPPORTED, "a batched table must run a blend-then-shift sweep (" +
                                        (c->stencil_ok ? std::string("its records do not fit")
                                                       : c->stencil_why) + ")");
-    if (!rc && tile_rows > 0) rc = pg_set_tile_rows(c, tile_rows);
     for (int64_t t = 0; !rc && t < ntidx; ++t)
         if (tidx[t] < 0 || tidx[t] >= c->kp.ncells)
             rc = fail(PG_EINVAL, "seed index outside the grid");

@@ -1040,6 +1040,62 @@ int batch_blocks_per_sm(int storage, size_t smem, int threads) {
     return 0;
 }
 
+template <typename S>
+static cudaError_t r_batch_attr() {
+    static uint64_t attr_set = 0;
+    const uint64_t attr_bit = device_bit();
+    if (attr_set & attr_bit) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_stencil_r_batch<S, kRCellsPerThread>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) attr_set |= attr_bit;
+    return e;
+}
+
+template <typename S>
+static int r_batch_occupancy(int threads, size_t smem) {
+    int nb = 0;
+    if (r_batch_attr<S>() != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_r_batch<S, kRCellsPerThread>,
+                                                      threads, smem) != cudaSuccess)
+        return 0;
+    return nb;
+}
+
+int r_batch_blocks_per_sm(int storage, size_t smem, int threads) {
+    switch (storage) {
+        case PG_STORE_F32: return r_batch_occupancy<float>(threads, smem);
+        case PG_STORE_F16: return r_batch_occupancy<__half>(threads, smem);
+        case PG_STORE_BF16: return r_batch_occupancy<__nv_bfloat16>(threads, smem);
+        case PG_STORE_Q16: return r_batch_occupancy<Q16>(threads, smem);
+    }
+    return 0;
+}
+
+cudaError_t launch_stencil_r_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
+                                   int64_t count, int threads, int parity, const int32_t* done,
+                                   double* part_sum, double* part_max, size_t smem, int grid,
+                                   cudaStream_t st) {
+    if (threads <= 0 || threads > RShape<kRCellsPerThread>::kMaxThreads || threads % 32 != 0 ||
+        grid <= 0 || smem > 200 * 1024)
+        return cudaErrorInvalidValue;
+#define PG_RB(S)                                                                                 \
+    {                                                                                            \
+        cudaError_t e = r_batch_attr<S>();                                                       \
+        if (e != cudaSuccess) return e;                                                          \
+        k_stencil_r_batch<S, kRCellsPerThread><<<grid, threads, smem, st>>>(                     \
+            tabs, ntab, first, count, parity, done, part_sum, part_max);                         \
+        return cudaGetLastError();                                                               \
+    }
+    switch (storage) {
+        case PG_STORE_F32: PG_RB(float);
+        case PG_STORE_F16: PG_RB(__half);
+        case PG_STORE_BF16: PG_RB(__nv_bfloat16);
+        case PG_STORE_Q16: PG_RB(Q16);
+    }
+#undef PG_RB
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const int32_t* order,
                                  uint16_t* gord, cudaStream_t st, int64_t* launches) {
     const size_t smem = stencil_group_smem(kp.nctl);

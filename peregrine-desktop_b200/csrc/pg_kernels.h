@@ -65,6 +65,11 @@ cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab
 cudaError_t launch_reduce_batch(const BatchTable* tabs, int ntab, const double* part_sum,
                                 const double* part_max, double* out, cudaStream_t st);
 int batch_blocks_per_sm(int storage, size_t smem, int threads);
+cudaError_t launch_stencil_r_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
+                                   int64_t count, int threads, int parity, const int32_t* done,
+                                   double* part_sum, double* part_max, size_t smem, int grid,
+                                   cudaStream_t st);
+int r_batch_blocks_per_sm(int storage, size_t smem, int threads);
 cudaError_t launch_adj_active(const float* V, const int16_t* pol, const uint8_t* occ,
                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                               uint8_t* active, cudaStream_t st);

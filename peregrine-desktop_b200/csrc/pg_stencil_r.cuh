@@ -231,12 +231,12 @@ __host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2, i
 // shared memory; the control loop then reads nothing else but the corner
 // values at the start of each group.
 template <typename S, bool ARGMIN, int KR>
-__global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
-    k_stencil_r(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
-                const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
-                const uint32_t* __restrict__ rctab, KParams kp, const uint16_t* __restrict__ gord,
-                double* part_sum, double* part_max, int16_t* argmin) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void stencil_r_item(
+    const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
+    const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
+    const uint32_t* __restrict__ rctab, const KParams& kp, const uint16_t* __restrict__ gord,
+    double* part_sum, double* part_max, int16_t* argmin, int64_t item, int64_t slot,
+    unsigned char* smem_raw) {
     const int nctl = kp.nctl;
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
     const int32_t TX = kp.tile_x;
@@ -260,7 +260,6 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
     load_grid(g, kp.g);
     const float cap = kp.p.cap;
     const int64_t P = L.P;
-    const int64_t item = blockIdx.x;
     const int64_t pl = item / kp.tiles_x;
     const int32_t xt = (int32_t)(item - pl * kp.tiles_x);
     const int32_t x0 = xt * TX;
@@ -353,6 +352,7 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
     }
     // mask word of cell slot q in a control's words; its bit is the lane
     const int32_t mw0 = tid >> 5;
+    const int32_t nq = (ncell + T - 1) / T;  // cell slots in use
     const uint32_t lane = (uint32_t)tid & 31u;
     __syncthreads();
 
@@ -443,6 +443,7 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         const uint32_t* mu = msk + u * MWS + mw0;
 #pragma unroll
         for (int q = 0; q < KR; ++q) {
+            if (q >= nq) break;  // block-uniform: slots no thread of the tile uses
             const int32_t a = caj[q] >> 16, j = caj[q] & 0xffff;
             const bool adm = ((live >> q) & (mu[q * mwq] >> lane)) & 1u;
             const int2 rr = ri[a];
@@ -492,5 +493,58 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
             Vo0[e] = ov;
         }
     }
-    block_partial_at(dsum, dmax, part_sum, part_max, item);
+    block_partial_at(dsum, dmax, part_sum, part_max, slot);
+}
+
+// The single-table sweep: one block per work item.
+template <typename S, bool ARGMIN, int KR>
+__global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
+    k_stencil_r(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
+                const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
+                const uint32_t* __restrict__ rctab, KParams kp, const uint16_t* __restrict__ gord,
+                double* part_sum, double* part_max, int16_t* argmin) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    stencil_r_item<S, ARGMIN, KR>(Vin, Vout, occ, recs, tmask, rctab, kp, gord, part_sum, part_max,
+                                  argmin, blockIdx.x, blockIdx.x, smem_raw);
+}
+
+// Many tables in one launch, as k_stencil_b_batch (pg_stencil_b.cuh) but
+// with the register-resident item: a persistent grid walks the items
+// [first, first + count) of the tables sharing one block size; items of a
+// table whose `done` flag is set only clear their residual slot.
+template <typename S, int KR>
+__global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
+    k_stencil_r_batch(const BatchTable* __restrict__ tabs, int ntab, int64_t first, int64_t count,
+                      int parity, const int32_t* __restrict__ done, double* part_sum,
+                      double* part_max) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) BatchTable tb;
+    __shared__ int cur;
+    if (threadIdx.x == 0) cur = -1;
+    for (int64_t it = first + blockIdx.x; it < first + count; it += gridDim.x) {
+        int lo = 0, hi = ntab - 1;  // the table owning item `it`
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tabs[mid].item0 <= it) lo = mid;
+            else hi = mid - 1;
+        }
+        __syncthreads();  // the previous item's shared memory is free
+        if (lo != cur) {
+            constexpr int nw = (int)(sizeof(BatchTable) / 4);
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(tabs + lo);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&tb);
+            for (int k = threadIdx.x; k < nw; k += blockDim.x) dst[k] = src[k];
+            __syncthreads();
+            if (threadIdx.x == 0) cur = lo;
+        }
+        if (done[lo]) {
+            if (threadIdx.x == 0) { part_sum[it] = 0.0; part_max[it] = 0.0; }
+            continue;
+        }
+        const S* vin = static_cast<const S*>(tb.V[parity]);
+        S* vout = const_cast<S*>(static_cast<const S*>(tb.V[1 - parity]));
+        stencil_r_item<S, false, KR>(vin, vout, tb.occ, tb.recs, tb.tmask, tb.rctab, tb.kp,
+                                     tb.gord, part_sum, part_max, nullptr, it - tb.item0, it,
+                                     smem_raw);
+    }
 }

@@ -75,6 +75,9 @@ struct BatchTable {
     const uint32_t* mask;
     const uint32_t* recs;
     const int32_t* order;
+    const uint32_t* tmask;   // register-resident sweep: tile-order mask
+    const uint32_t* rctab;   // register-resident sweep: successor entries
+    const uint16_t* gord;    // register-resident sweep: group order
     int64_t item0, nitems;
     int32_t vec;
     int32_t pad;
