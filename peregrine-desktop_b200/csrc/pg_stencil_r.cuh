@@ -276,6 +276,52 @@ __device__ __forceinline__ void stencil_r_item(
     }
     const uint32_t* prec = recs + (size_t)pl * nctl * kURec;
 
+    // stage the block's per-control data
+    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
+    for (int i = tid; i < nctl * kRWt; i += T) {
+        const int u = i / kRWt, f = i - u * kRWt;
+        const uint32_t* rec = prec + (size_t)u * kURec;
+        // w[16], tau, ok, ox, oy
+        const int sf = f < 17 ? f : (f == 17 ? kUNT + 18 : (f == 18 ? kUNT + 16 : kUNT + 17));
+        const uint32_t v = __ldg(rec + sf);
+        wt[i] = __uint_as_float(v);
+    }
+    {
+        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * MW;
+        for (int i = tid; i < nctl * MWS; i += T) {
+            const int u = i / MWS, w = i - u * MWS;
+            msk[i] = w < MW ? __ldg(src + (size_t)u * MW + w) : 0u;
+        }
+    }
+    __syncthreads();  // wt
+    {
+        const int32_t per = nr + n2;
+        for (int32_t i = tid; i < nctl * per; i += T) {
+            const int32_t u = i / per, it = i - u * per;
+            if (__float_as_uint(wt[u * kRWt + 17]) == 0u) continue;  // never read
+            const bool row = it < nr;
+            const int32_t idx = row ? x0 + it : it - nr;
+            const uint32_t e =
+                __ldg(rctab + ((size_t)pl * nctl + u) * (n1 + n2) + (row ? idx : n1 + idx));
+            const int32_t off = __float_as_int(wt[u * kRWt + (row ? 18 : 19)]);
+            int32_t li;
+            float t;
+            if ((e & kRcSlow) == kRcSlow) {
+                const uint32_t* rec = prec + (size_t)u * kURec;
+                const float* inc =
+                    reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
+                succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
+            } else {
+                li = idx + off - 1 + (int32_t)(e >> 30);
+                t = __uint_as_float(e & ~kRcSlow);
+            }
+            const int32_t wbase = x0 + off - 1;
+            rcinfo[(size_t)u * rcs + (row ? it : TX + it - nr)] =
+                row ? make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t))
+                    : make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
+        }
+    }
+
     // this thread's tile cells e = tid + q*T: (row a, column j) packed
     const uint8_t* occ_h = occ + ((int64_t)pq6[0] * n1 + x0) * n2;
     float best[KR];
@@ -308,12 +354,15 @@ __device__ __forceinline__ void stencil_r_item(
     const int32_t mw0 = tid >> 5;
     const int32_t nq = (ncell + T - 1) / T;  // cell slots in use
     const uint32_t lane = (uint32_t)tid & 31u;
+    __syncthreads();
+
     static_assert(KR % 2 == 0, "window slots are paired for the packed FMA");
     uint64_t cv[KR / 2][16];  // the group's corner values, slots 2i and 2i+1 paired
-    // corner values of the group that control u starts: the planes of its
-    // record, rows from its x offset ox
-    auto load_group = [&](int u, int32_t ox) {
-        const int32_t wbase = x0 + ox - 1;
+    // corner values of the group that control uu starts: the planes of its
+    // record, rows from its x offset
+    auto load_group = [&](int uu) {
+        const int u = ord[uu] & 0x7fff;
+        const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 18]) - 1;
         const uint32_t* rec = prec + (size_t)u * kURec;
         const S* base[KR];
 #pragma unroll
@@ -330,62 +379,9 @@ __device__ __forceinline__ void stencil_r_item(
                 cv[k / 2][c] = pk2(Conv<S>::ld(base[k] + off), Conv<S>::ld(base[k + 1] + off));
         }
     };
-    // the first control starts a group (inadmissible controls come last and
-    // their records' corner planes are never read): its loads are issued
-    // before the staging below and fly while it runs
-    {
-        const int u0 = __ldg(gord + (size_t)pl * nctl) & 0x7fff;
-        const uint32_t* rec0 = prec + (size_t)u0 * kURec;
-        if (__ldg(rec0 + kUNT + 18) != 0u) load_group(u0, (int32_t)__ldg(rec0 + kUNT + 16));
-    }
-    // stage the block's per-control data, one warp per control
-    const int warp = tid >> 5, nwarp = T >> 5;
-    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
-    {
-        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * MW;
-        for (int u = warp; u < nctl; u += nwarp) {
-            const uint32_t* rec = prec + (size_t)u * kURec;
-            if ((int)lane < kRWt) {
-                // w[16], tau, ok, ox, oy
-                const int f = (int)lane;
-                const int sf = f < 17 ? f : (f == 17 ? kUNT + 18 : (f == 18 ? kUNT + 16 : kUNT + 17));
-                wt[u * kRWt + f] = __uint_as_float(__ldg(rec + sf));
-            }
-            for (int w = (int)lane; w < MWS; w += 32)
-                msk[u * MWS + w] = w < MW ? __ldg(src + (size_t)u * MW + w) : 0u;
-        }
-    }
-    __syncthreads();  // wt
-    for (int u = warp; u < nctl; u += nwarp) {
-        if (__float_as_uint(wt[u * kRWt + 17]) == 0u) continue;  // never read
-        const int32_t offx = __float_as_int(wt[u * kRWt + 18]);
-        const int32_t offy = __float_as_int(wt[u * kRWt + 19]);
-        const uint32_t* rrow = rctab + ((size_t)pl * nctl + u) * (n1 + n2);
-        for (int32_t it = (int32_t)lane; it < nr + n2; it += 32) {
-            const bool row = it < nr;
-            const int32_t idx = row ? x0 + it : it - nr;
-            const uint32_t e = __ldg(rrow + (row ? idx : n1 + idx));
-            const int32_t off = row ? offx : offy;
-            int32_t li;
-            float t;
-            if ((e & kRcSlow) == kRcSlow) {
-                const uint32_t* rec = prec + (size_t)u * kURec;
-                const float* inc =
-                    reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
-                succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
-            } else {
-                li = idx + off - 1 + (int32_t)(e >> 30);
-                t = __uint_as_float(e & ~kRcSlow);
-            }
-            const int32_t wbase = x0 + offx - 1;
-            rcinfo[(size_t)u * rcs + (row ? it : TX + it - nr)] =
-                row ? make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t))
-                    : make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
-        }
-    }
-
-    __syncthreads();
-
+    // the first control starts a group; inadmissible controls come last and
+    // their records' corner planes are never read
+    if (__float_as_uint(wt[(ord[0] & 0x7fff) * kRWt + 17]) != 0u) load_group(0);
     int buf = 0;
     for (int uu = 0; uu < nctl; ++uu) {
         const uint32_t ent = ord[uu];
@@ -433,11 +429,9 @@ __device__ __forceinline__ void stencil_r_item(
         }
         // the corner values are free now: if the next control starts a new
         // group, its loads fly during this control's barrier and phase 2
-        if (uu + 1 < nctl && (ord[uu + 1] & kGroupFirst)) {
-            const int un = ord[uu + 1] & 0x7fff;
-            if (__float_as_uint(wt[un * kRWt + 17]) != 0u)
-                load_group(un, __float_as_int(wt[un * kRWt + 18]));
-        }
+        if (uu + 1 < nctl && (ord[uu + 1] & kGroupFirst) &&
+            __float_as_uint(wt[(ord[uu + 1] & 0x7fff) * kRWt + 17]) != 0u)
+            load_group(uu + 1);
         __syncthreads();
 
         // phase 2: shift, admissibility, tau, min -- computed for every cell
