@@ -85,7 +85,8 @@ struct pg_ctx {
     bool blend_ok = false;   // the blend-then-shift tiling fits (shared memory, row width)
     bool gather_ok = false;  // the 64-corner masked gather fits its shared memory
     uint16_t* gord_d = nullptr;  // per plane, its controls in corner-group order
-    uint32_t* rctab_d = nullptr; // per (plane, control, row / column), successor entries
+    int2* rctab_d = nullptr;     // per (plane, control): its row, then column successor
+                                 // entries (rows for the current tiling)
     uint32_t* tmask_d = nullptr; // admissibility per (plane, tile, control) in tile order
     size_t tmask_cap = 0;
     bool rblend_ok = false;      // the register-resident blend can run (tables, tiling)
@@ -215,12 +216,18 @@ void r_tiling(pg::KParams& kp, int32_t rows) {
 }
 
 // The register-resident blend keeps every control's successor corners in
-// shared memory; it runs where that leaves room for two blocks per SM (or,
+// shared memory; it runs where that leaves room for two blocks per SM (228 KB
+// of shared memory per SM less 1 KB reserved per block; or,
 // with more than 256 threads, the block has the SM to itself anyway) and the
 // re-reading blend runs elsewhere.
+// The column entries follow the row entries in rctab_d.
+const int2* r_cols(const pg_ctx* ctx) {
+    return ctx->rctab_d + (size_t)ctx->kp.nplanes * ctx->kp.nctl * ctx->kp.g.n[0];
+}
+
 bool r_smem_fits(const pg::KParams& kp) {
     return kp.rtile_x > 0 &&
-           pg::stencil_r_smem_bytes(kp) <= (size_t)(kp.rblock > 256 ? 200 : 100) * 1024;
+           pg::stencil_r_smem_bytes(kp) <= (size_t)(kp.rblock > 256 ? 200 : 110) * 1024;
 }
 
 // (Re)builds the tile-order mask of the register-resident blend for the
@@ -231,6 +238,15 @@ int build_r_tables(pg_ctx* ctx) {
     pg::KParams& kp = ctx->kp;
     ctx->rblend_ok = false;
     if (!ctx->mask_ok || !ctx->gord_d || !ctx->rctab_d || !r_smem_fits(kp)) return PG_OK;
+    // the successor entries (their row form depends on the tiling)
+    {
+        int2* rrow = ctx->rctab_d;
+        int2* rcol = rrow + (size_t)kp.nplanes * kp.nctl * kp.g.n[0];
+        cudaError_t e = pg::launch_stencil_rc(ctx->recs_d, kp, rrow, rcol, ctx->stream,
+                                              &ctx->launches);
+        if (e != cudaSuccess)
+            return fail(PG_ECUDA, std::string("successor table: ") + cudaGetErrorString(e));
+    }
     const size_t need = pg::stencil_tmask_bytes(kp);
     if (need > ctx->tmask_cap) {
         PG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -290,8 +306,8 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
                                 ctx->stream, &ctx->launches);
     else if (kernel == PG_KERNEL_STENCIL && r_ok)
         e = pg::launch_stencil_r(ctx->storage, vin, vout, ctx->occ_d, ctx->recs_d, ctx->tmask_d,
-                                 ctx->rctab_d, ctx->kp, ctx->gord_d, sb, argmin_d, ctx->stream,
-                                 &ctx->launches);
+                                 ctx->rctab_d, r_cols(ctx), ctx->kp, ctx->gord_d, sb, argmin_d,
+                                 ctx->stream, &ctx->launches);
     else if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_BLEND) && b_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  ctx->kp, ctx->order_d, sb, argmin_d, ctx->stream,
@@ -615,9 +631,6 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
                 cudaMalloc(&ctx->rctab_d, rcb) == cudaSuccess) {
                 e = pg::launch_stencil_group(ctx->recs_d, kp, ctx->order_d, ctx->gord_d,
                                              ctx->stream, &ctx->launches);
-                if (e == cudaSuccess)
-                    e = pg::launch_stencil_rc(ctx->recs_d, kp, ctx->rctab_d, ctx->stream,
-                                              &ctx->launches);
                 if (e != cudaSuccess)
                     return fail(PG_ECUDA, std::string("group: ") + cudaGetErrorString(e));
                 int rc2 = build_r_tables(ctx);
@@ -938,8 +951,8 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
     void* spare = ctx->V[1 - ctx->cur];
     if (ctx->rblend_ok)
         e = pg::launch_stencil_r(ctx->storage, vin, spare, ctx->occ_d, ctx->recs_d, ctx->tmask_d,
-                                 ctx->rctab_d, kp, ctx->gord_d, sb, ctx->argmin_d, ctx->stream,
-                                 &ctx->launches);
+                                 ctx->rctab_d, r_cols(ctx), kp, ctx->gord_d, sb, ctx->argmin_d,
+                                 ctx->stream, &ctx->launches);
     else if (ctx->blend_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  kp, ctx->order_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
@@ -1157,7 +1170,8 @@ int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, std::
         t.recs = c->recs_d;
         t.order = c->order_d;
         t.tmask = c->tmask_d;
-        t.rctab = c->rctab_d;
+        t.rrow = c->rctab_d;
+        t.rcol = c->rctab_d ? r_cols(c) : nullptr;
         t.gord = c->gord_d;
         t.kp = c->kp;
         t.kp.tile_x = use_r ? c->kp.rtile_x : c->kp.btile_x;

@@ -1116,9 +1116,10 @@ cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const 
 
 template <typename S, bool ARGMIN, int KR>
 static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
-                               const uint32_t* recs, const uint32_t* tmask, const uint32_t* rctab,
-                               const KParams& kp, const uint16_t* gord, const SweepBufs& sb,
-                               int16_t* argmin, cudaStream_t st, int64_t* launches) {
+                               const uint32_t* recs, const uint32_t* tmask, const int2* rrow,
+                               const int2* rcol, const KParams& kp, const uint16_t* gord,
+                               const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                               int64_t* launches) {
     if (kp.rtile_x <= 0 || kp.rblock <= 0 || kp.rblock > RShape<KR>::kMaxThreads ||
         kp.rblock % 32 != 0 || kp.nsub > kStencilMaxSub || kp.g.n[1] > 0xffff ||
         (int64_t)(kp.rtile_x + 3) * kp.g.n[1] > (int64_t)kp.rblock * KR)
@@ -1139,7 +1140,7 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
         attr_set |= attr_bit;
     }
     k_stencil_r<S, ARGMIN, KR><<<(unsigned)blocks, kp.rblock, smem, st>>>(
-        (const S*)Vin, (S*)Vout, occ, recs, tmask, rctab, kr, gord, sb.part_sum, sb.part_max,
+        (const S*)Vin, (S*)Vout, occ, recs, tmask, rrow, rcol, kr, gord, sb.part_sum, sb.part_max,
         argmin);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1149,14 +1150,17 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
 }
 
 cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uint8_t* occ,
-                             const uint32_t* recs, const uint32_t* tmask, const uint32_t* rctab,
-                             const KParams& kp, const uint16_t* gord, const SweepBufs& sb,
-                             int16_t* argmin, cudaStream_t st, int64_t* launches) {
+                             const uint32_t* recs, const uint32_t* tmask, const int2* rrow,
+                             const int2* rcol, const KParams& kp, const uint16_t* gord,
+                             const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                             int64_t* launches) {
 #define PG_SR(S)                                                                                 \
-    return argmin ? stencil_r_t<S, true, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rctab,   \
-                                                           kp, gord, sb, argmin, st, launches)   \
-                  : stencil_r_t<S, false, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rctab,  \
-                                                            kp, gord, sb, argmin, st, launches)
+    return argmin ? stencil_r_t<S, true, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rrow,    \
+                                                           rcol, kp, gord, sb, argmin, st,       \
+                                                           launches)                             \
+                  : stencil_r_t<S, false, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rrow,   \
+                                                            rcol, kp, gord, sb, argmin, st,      \
+                                                            launches)
     switch (storage) {
         case PG_STORE_F32: PG_SR(float);
         case PG_STORE_F16: PG_SR(__half);
@@ -1167,10 +1171,11 @@ cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uin
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_stencil_rc(const uint32_t* recs, const KParams& kp, uint32_t* rctab,
+cudaError_t launch_stencil_rc(const uint32_t* recs, const KParams& kp, int2* rrow, int2* rcol,
                               cudaStream_t st, int64_t* launches) {
+    if (kp.rtile_x <= 0) return cudaErrorInvalidValue;
     const int64_t total = kp.nplanes * kp.nctl * (kp.g.n[0] + kp.g.n[1]);
-    k_stencil_rc<<<grid_for(total, 256), 256, 0, st>>>(recs, kp, rctab);
+    k_stencil_rc<<<grid_for(total, 256), 256, 0, st>>>(recs, kp, kp.rtile_x, rrow, rcol);
     *launches += 1;
     return cudaGetLastError();
 }
@@ -1179,17 +1184,24 @@ cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, uint32
                                  cudaStream_t st, int64_t* launches) {
     if (kp.rtile_x <= 0) return cudaErrorInvalidValue;
     const int64_t total = stencil_tmask_bytes(kp) / 4;
-    k_stencil_tmask<<<grid_for(total, 256), 256, 0, st>>>(mask, kp, kp.rtile_x, kp.rtiles_x, tmask);
+    k_stencil_tmask<<<grid_for(total, 256), 256, 0, st>>>(mask, kp, kp.rtile_x, kp.rtiles_x,
+                                                          stencil_r_mask_words(kp), tmask);
     *launches += 1;
     return cudaGetLastError();
 }
 
 size_t stencil_rc_bytes(const KParams& kp) {
-    return (size_t)kp.nplanes * kp.nctl * (kp.g.n[0] + kp.g.n[1]) * sizeof(uint32_t);
+    return (size_t)kp.nplanes * kp.nctl * (kp.g.n[0] + kp.g.n[1]) * sizeof(int2);
+}
+
+// mask words per control of the register-resident sweep: one per warp and
+// cell slot
+int32_t stencil_r_mask_words(const KParams& kp) {
+    return kRCellsPerThread * (kp.rblock / 32);
 }
 
 size_t stencil_tmask_bytes(const KParams& kp) {
-    return (size_t)kp.nplanes * kp.rtiles_x * kp.nctl * tile_mask_words(kp.rtile_x, kp.g.n[1]) *
+    return (size_t)kp.nplanes * kp.rtiles_x * kp.nctl * stencil_r_mask_words(kp) *
            sizeof(uint32_t);
 }
 

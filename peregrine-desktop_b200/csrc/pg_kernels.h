@@ -48,11 +48,13 @@ size_t stencil_b_smem_bytes(const KParams& kp);
 cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const int32_t* order,
                                  uint16_t* gord, cudaStream_t st, int64_t* launches);
 cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uint8_t* occ,
-                             const uint32_t* recs, const uint32_t* tmask, const uint32_t* rctab,
-                             const KParams& kp, const uint16_t* gord, const SweepBufs& sb,
-                             int16_t* argmin, cudaStream_t st, int64_t* launches);
-cudaError_t launch_stencil_rc(const uint32_t* recs, const KParams& kp, uint32_t* rctab,
+                             const uint32_t* recs, const uint32_t* tmask, const int2* rrow,
+                             const int2* rcol, const KParams& kp, const uint16_t* gord,
+                             const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                             int64_t* launches);
+cudaError_t launch_stencil_rc(const uint32_t* recs, const KParams& kp, int2* rrow, int2* rcol,
                               cudaStream_t st, int64_t* launches);
+int32_t stencil_r_mask_words(const KParams& kp);
 cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, uint32_t* tmask,
                                  cudaStream_t st, int64_t* launches);
 size_t stencil_r_smem_bytes(const KParams& kp);

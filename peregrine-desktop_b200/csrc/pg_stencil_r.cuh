@@ -14,18 +14,19 @@
 //   (corner planes, x offset) and flags the first control of each group;
 //   controls that no cell of the plane admits go last;
 //
-//   k_stencil_rc (once per solve) stores each (plane, control, row or
-//   column)'s successor corner and fraction, which k_stencil_b recomputes
-//   every sweep, and k_stencil_tmask (once per tiling) regroups the
-//   admissibility mask per (plane, tile, control) in tile order;
+//   k_stencil_rc (once per tiling) stores each (plane, control, row)'s and
+//   each (plane, control, column)'s successor corner and fraction -- which
+//   k_stencil_b recomputes every sweep -- in the form the sweep reads them,
+//   and k_stencil_tmask (once per tiling) regroups the admissibility mask per
+//   (plane, tile, control) in tile order;
 //
-//   k_stencil_r stages a block's per-control data (weights, tau, mask words,
-//   successor entries) in shared memory, loads at the first control of each
-//   group the 16 corner values of each of its window cells into registers
-//   (KR cells per thread), and for every control of the group blends them
-//   with the control's 16 weights -- 16 FMAs per window cell from registers,
-//   nothing re-read -- into the shared window, then shifts exactly as
-//   k_stencil_b does.
+//   k_stencil_r copies a block's per-control data (weights, tau, offsets,
+//   mask words, successor entries) into shared memory with asynchronous
+//   copies, loads at the first control of each group the 16 corner values
+//   of each of its window cells into registers (KR cells per thread), and
+//   for every control of the group blends them with the control's 16
+//   weights -- 16 FMAs per window cell from registers, nothing re-read --
+//   into the shared window, then shifts exactly as k_stencil_b does.
 //
 // The arithmetic is k_stencil_b's, operation for operation: the same FMA
 // chain over the corners in record order, the same per-row / per-column
@@ -132,19 +133,16 @@ __device__ __forceinline__ void succ_li_t(const GridT<float>& g, const float* in
     *li = (int32_t)fminf(fmaxf(fl, -2.0f), (float)(row ? n1 + 2 : n2 + 2));
 }
 
-// Packed successor entry of a (plane, control, row or column): the fraction
-// t in bits 0-29 (t is in [0, 1), so its sign and top exponent bit are 0)
-// and d = li - idx - (offset - 1) in bits 30-31, where offset is the
-// control's nominal x (rows) or y (columns) offset; d = 3 marks an entry
-// outside offset - 1 .. offset + 1 (or a t out of range), which the sweep
-// recomputes.
-constexpr uint32_t kRcSlow = 3u << 30;
-
-// Once per solve: the packed entries of every (plane, control), n1 rows
-// then n2 columns.  Inadmissible controls get 0 (never read).
-__global__ void k_stencil_rc(const uint32_t* __restrict__ recs, KParams kp,
-                             uint32_t* __restrict__ rctab) {
-    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], per = n1 + n2;
+// Once per tiling: the successor entries of every (plane, control) in the
+// form the sweep reads them.  Rows (rrow, n1 per pair): (window offset, x
+// fraction), the window offset = (li - wbase) clamped to the window of the
+// row's tile, times the window row stride n2 + 1, with wbase = x0 + ox - 1
+// for the tile's first row x0 and the control's nominal x offset ox.
+// Columns (rcol, n2 per pair): (li clamped to the columns, y fraction).
+// Inadmissible controls get (0, 0), never read.
+__global__ void k_stencil_rc(const uint32_t* __restrict__ recs, KParams kp, int32_t tile_x,
+                             int2* __restrict__ rrow, int2* __restrict__ rcol) {
+    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], per = n1 + n2, SB = n2 + 1;
     GridT<float> g;
     load_grid(g, kp.g);
     const int64_t total = kp.nplanes * kp.nctl * per;
@@ -152,21 +150,26 @@ __global__ void k_stencil_rc(const uint32_t* __restrict__ recs, KParams kp,
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pu = i / per;
         const int32_t it = (int32_t)(i - pu * per);
-        const uint32_t* rec = recs + (size_t)pu * kURec;
-        if (__ldg(rec + kUNT + 18) == 0u) {
-            rctab[i] = 0u;
-            continue;
-        }
         const bool row = it < n1;
         const int32_t idx = row ? it : it - n1;
-        const int32_t off = (int32_t)__ldg(rec + kUNT + (row ? 16 : 17));
+        int2* dst = row ? rrow + pu * n1 + idx : rcol + pu * n2 + idx;
+        const uint32_t* rec = recs + (size_t)pu * kURec;
+        if (__ldg(rec + kUNT + 18) == 0u) {
+            *dst = make_int2(0, 0);
+            continue;
+        }
         const float* inc = reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
         int32_t li;
         float t;
         succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
-        const int32_t d = li - idx - off + 1;
-        const uint32_t tb = __float_as_uint(t);
-        rctab[i] = (d >= 0 && d <= 2 && t >= 0.0f && t < 1.0f) ? ((uint32_t)d << 30) | tb : kRcSlow;
+        if (row) {
+            const int32_t x0 = (idx / tile_x) * tile_x;
+            const int32_t nw = min(tile_x, n1 - x0) + 3;
+            const int32_t wbase = x0 + (int32_t)__ldg(rec + kUNT + 16) - 1;
+            *dst = make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t));
+        } else {
+            *dst = make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
+        }
     }
 }
 
@@ -177,17 +180,17 @@ __host__ __device__ inline int32_t tile_mask_words(int32_t tile_x, int32_t n2) {
 }
 
 // Once per tiling: the admissibility mask regrouped per (plane, tile,
-// control) in tile order, from the per-row layout of k_stencil_prep.
+// control) in tile order, from the per-row layout of k_stencil_prep; mws
+// words per control (the sweep's words per control, zero past the tile).
 __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, int32_t tile_x,
-                                int32_t tiles_x, uint32_t* __restrict__ tmask) {
+                                int32_t tiles_x, int32_t mws, uint32_t* __restrict__ tmask) {
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], W = mask_words(n2);
-    const int32_t MW = tile_mask_words(tile_x, n2);
     const int nctl = kp.nctl;
-    const int64_t total = kp.nplanes * tiles_x * nctl * MW;
+    const int64_t total = kp.nplanes * tiles_x * nctl * mws;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t r = i / MW;
-        const int32_t w = (int32_t)(i - r * MW);
+        int64_t r = i / mws;
+        const int32_t w = (int32_t)(i - r * mws);
         const int32_t u = (int32_t)(r % nctl);
         r /= nctl;
         const int32_t xt = (int32_t)(r % tiles_x);
@@ -207,12 +210,12 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
 }
 
 // Shared memory of one k_stencil_r block of `threads` threads (a multiple of
-// 32) with KR cells per thread: the plane's group order; per control its 16
-// weights, tau, admissibility and x / y offsets (20 words), its mask words
-// (one per warp and cell slot: the tile's words, zero beyond them) and its
-// successor entries; and two padded window buffers with room for every
-// thread's KR window slots (slots past the window land in scratch rows).
-constexpr int kRWt = 20;
+// 32) with KR cells per thread: the plane's group order; per control its
+// record's weights, tau, offsets, admissibility and substeps (24 words), its
+// mask words (one per warp and cell slot: the tile's words, zero beyond them)
+// and its successor entries; and two padded window buffers with room for
+// every thread's KR window slots (slots past the window land in scratch rows).
+constexpr int kRWt = 24;  // w[16], tau, tx, ty, -, ox, oy, ok, nsub
 __host__ __device__ inline int32_t stencil_r_window_rows(int tile_x, int n2, int threads, int kr) {
     const int32_t slots = (kr * threads + n2 - 1) / n2;
     return slots > tile_x + 3 ? slots : tile_x + 3;
@@ -234,9 +237,9 @@ template <typename S, bool ARGMIN, int KR>
 __device__ __forceinline__ void stencil_r_item(
     const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
     const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
-    const uint32_t* __restrict__ rctab, const KParams& kp, const uint16_t* __restrict__ gord,
-    double* part_sum, double* part_max, int16_t* argmin, int64_t item, int64_t slot,
-    unsigned char* smem_raw) {
+    const int2* __restrict__ rrow, const int2* __restrict__ rcol, const KParams& kp,
+    const uint16_t* __restrict__ gord, double* part_sum, double* part_max, int16_t* argmin,
+    int64_t item, int64_t slot, unsigned char* smem_raw) {
     const int nctl = kp.nctl;
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
     const int32_t TX = kp.tile_x;
@@ -244,7 +247,6 @@ __device__ __forceinline__ void stencil_r_item(
     const int tid = threadIdx.x;
     const int32_t SB = n2 + 1;  // window row stride (one padding column)
     const int32_t bsz = stencil_r_window_rows(TX, n2, T, KR) * SB;
-    const int32_t MW = tile_mask_words(TX, n2);
     const int32_t mwq = T >> 5;          // mask words per cell slot
     const int32_t MWS = KR * mwq;        // mask words per control in shared memory
     const int32_t rcs = TX + n2;  // successor entries per control
@@ -256,8 +258,6 @@ __device__ __forceinline__ void stencil_r_item(
     int2* rcinfo = reinterpret_cast<int2*>(msk + nctl * MWS + ((nctl * MWS) & 1));
     float* Bbuf = reinterpret_cast<float*>(rcinfo + nctl * rcs);
     const Layout L = make_layout(kp);
-    GridT<float> g;
-    load_grid(g, kp.g);
     const float cap = kp.p.cap;
     const int64_t P = L.P;
     const int64_t pl = item / kp.tiles_x;
@@ -265,7 +265,6 @@ __device__ __forceinline__ void stencil_r_item(
     const int32_t x0 = xt * TX;
     const int32_t nr = min(TX, n1 - x0);
     const int32_t ncell = nr * n2;
-    const int32_t nw = nr + 3;  // window rows x0+ox-1 .. x0+ox+nr+1
     int32_t pq6[4];
     {
         int64_t pp = pl;
@@ -276,51 +275,30 @@ __device__ __forceinline__ void stencil_r_item(
     }
     const uint32_t* prec = recs + (size_t)pl * nctl * kURec;
 
-    // stage the block's per-control data
+    // stage the block's per-control data with asynchronous copies, waited
+    // for once below: per control its record's words 0-19 (w[16], tau, tx,
+    // ty, -) and kUNT+16..19 (ox, oy, ok, nsub) as six 16-byte pieces, its
+    // mask words, its row and column successor entries
     for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
-    for (int i = tid; i < nctl * kRWt; i += T) {
-        const int u = i / kRWt, f = i - u * kRWt;
-        const uint32_t* rec = prec + (size_t)u * kURec;
-        // w[16], tau, ok, ox, oy
-        const int sf = f < 17 ? f : (f == 17 ? kUNT + 18 : (f == 18 ? kUNT + 16 : kUNT + 17));
-        const uint32_t v = __ldg(rec + sf);
-        wt[i] = __uint_as_float(v);
+    for (int i = tid; i < nctl * 6; i += T) {
+        const int u = i / 6, c = i - u * 6;
+        cp_async16(wt + u * kRWt + 4 * c, prec + (size_t)u * kURec + (c < 5 ? 4 * c : kUNT + 16));
     }
     {
-        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * MW;
-        for (int i = tid; i < nctl * MWS; i += T) {
-            const int u = i / MWS, w = i - u * MWS;
-            msk[i] = w < MW ? __ldg(src + (size_t)u * MW + w) : 0u;
-        }
+        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * MWS;
+        for (int i = tid; i < nctl * MWS / 4; i += T) cp_async16(msk + 4 * i, src + 4 * i);
     }
-    __syncthreads();  // wt
     {
         const int32_t per = nr + n2;
         for (int32_t i = tid; i < nctl * per; i += T) {
             const int32_t u = i / per, it = i - u * per;
-            if (__float_as_uint(wt[u * kRWt + 17]) == 0u) continue;  // never read
             const bool row = it < nr;
-            const int32_t idx = row ? x0 + it : it - nr;
-            const uint32_t e =
-                __ldg(rctab + ((size_t)pl * nctl + u) * (n1 + n2) + (row ? idx : n1 + idx));
-            const int32_t off = __float_as_int(wt[u * kRWt + (row ? 18 : 19)]);
-            int32_t li;
-            float t;
-            if ((e & kRcSlow) == kRcSlow) {
-                const uint32_t* rec = prec + (size_t)u * kURec;
-                const float* inc =
-                    reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
-                succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
-            } else {
-                li = idx + off - 1 + (int32_t)(e >> 30);
-                t = __uint_as_float(e & ~kRcSlow);
-            }
-            const int32_t wbase = x0 + off - 1;
-            rcinfo[(size_t)u * rcs + (row ? it : TX + it - nr)] =
-                row ? make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t))
-                    : make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
+            const int2* src = row ? rrow + ((size_t)pl * nctl + u) * n1 + x0 + it
+                                  : rcol + ((size_t)pl * nctl + u) * n2 + (it - nr);
+            cp_async8(rcinfo + (size_t)u * rcs + (row ? it : TX + it - nr), src);
         }
     }
+    cp_async_commit();
 
     // this thread's tile cells e = tid + q*T: (row a, column j) packed
     const uint8_t* occ_h = occ + ((int64_t)pq6[0] * n1 + x0) * n2;
@@ -354,6 +332,7 @@ __device__ __forceinline__ void stencil_r_item(
     const int32_t mw0 = tid >> 5;
     const int32_t nq = (ncell + T - 1) / T;  // cell slots in use
     const uint32_t lane = (uint32_t)tid & 31u;
+    cp_async_wait_all();
     __syncthreads();
 
     static_assert(KR % 2 == 0, "window slots are paired for the packed FMA");
@@ -362,7 +341,7 @@ __device__ __forceinline__ void stencil_r_item(
     // record, rows from its x offset
     auto load_group = [&](int uu) {
         const int u = ord[uu] & 0x7fff;
-        const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 18]) - 1;
+        const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 20]) - 1;
         const uint32_t* rec = prec + (size_t)u * kURec;
         const S* base[KR];
 #pragma unroll
@@ -381,13 +360,13 @@ __device__ __forceinline__ void stencil_r_item(
     };
     // the first control starts a group; inadmissible controls come last and
     // their records' corner planes are never read
-    if (__float_as_uint(wt[(ord[0] & 0x7fff) * kRWt + 17]) != 0u) load_group(0);
+    if (__float_as_uint(wt[(ord[0] & 0x7fff) * kRWt + 22]) != 0u) load_group(0);
     int buf = 0;
     for (int uu = 0; uu < nctl; ++uu) {
         const uint32_t ent = ord[uu];
         const int u = (int)(ent & 0x7fffu);
         const float* wu = wt + u * kRWt;
-        if (__float_as_uint(wu[17]) == 0u) {
+        if (__float_as_uint(wu[22]) == 0u) {
             // no cell of the plane admits this control (block-uniform)
             if constexpr (ARGMIN) {
 #pragma unroll
@@ -430,7 +409,7 @@ __device__ __forceinline__ void stencil_r_item(
         // the corner values are free now: if the next control starts a new
         // group, its loads fly during this control's barrier and phase 2
         if (uu + 1 < nctl && (ord[uu + 1] & kGroupFirst) &&
-            __float_as_uint(wt[(ord[uu + 1] & 0x7fff) * kRWt + 17]) != 0u)
+            __float_as_uint(wt[(ord[uu + 1] & 0x7fff) * kRWt + 22]) != 0u)
             load_group(uu + 1);
         __syncthreads();
 
@@ -501,11 +480,12 @@ template <typename S, bool ARGMIN, int KR>
 __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
     k_stencil_r(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
                 const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
-                const uint32_t* __restrict__ rctab, KParams kp, const uint16_t* __restrict__ gord,
-                double* part_sum, double* part_max, int16_t* argmin) {
+                const int2* __restrict__ rrow, const int2* __restrict__ rcol, KParams kp,
+                const uint16_t* __restrict__ gord, double* part_sum, double* part_max,
+                int16_t* argmin) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    stencil_r_item<S, ARGMIN, KR>(Vin, Vout, occ, recs, tmask, rctab, kp, gord, part_sum, part_max,
-                                  argmin, blockIdx.x, blockIdx.x, smem_raw);
+    stencil_r_item<S, ARGMIN, KR>(Vin, Vout, occ, recs, tmask, rrow, rcol, kp, gord, part_sum,
+                                  part_max, argmin, blockIdx.x, blockIdx.x, smem_raw);
 }
 
 // Many tables in one launch, as k_stencil_b_batch (pg_stencil_b.cuh) but
@@ -543,8 +523,8 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         }
         const S* vin = static_cast<const S*>(tb.V[parity]);
         S* vout = const_cast<S*>(static_cast<const S*>(tb.V[1 - parity]));
-        stencil_r_item<S, false, KR>(vin, vout, tb.occ, tb.recs, tb.tmask, tb.rctab, tb.kp,
-                                     tb.gord, part_sum, part_max, nullptr, it - tb.item0, it,
-                                     smem_raw);
+        stencil_r_item<S, false, KR>(vin, vout, tb.occ, tb.recs, tb.tmask, tb.rrow, tb.rcol,
+                                     tb.kp, tb.gord, part_sum, part_max, nullptr, it - tb.item0,
+                                     it, smem_raw);
     }
 }
