@@ -199,11 +199,23 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
         const int32_t ncell = min(tile_x, n1 - x0) * n2;
         const uint32_t* mrow = mask + ((size_t)pl * nctl + u) * n1 * W;
         uint32_t word = 0;
-        int32_t e = 32 * w;
+        // bits 32w .. 32w+31 of the tile: runs of consecutive columns of one
+        // row, each taken from at most two of the row's words
+        const int32_t e0 = 32 * w, e1 = min(e0 + 32, ncell);
+        int32_t e = e0;
         int32_t a = e / n2, j = e - a * n2;
-        for (int b = 0; b < 32 && e < ncell; ++b, ++e) {
-            word |= ((__ldg(mrow + (x0 + a) * W + (j >> 5)) >> (j & 31)) & 1u) << b;
-            if (++j == n2) { j = 0; ++a; }
+        while (e < e1) {
+            const int32_t len = min(e1 - e, n2 - j);  // 1..32
+            const uint32_t* rw = mrow + (x0 + a) * W;
+            const int32_t wi = j >> 5;
+            const uint32_t lo = __ldg(rw + wi);
+            const uint32_t hi = (wi + 1 < W) ? __ldg(rw + wi + 1) : 0u;
+            const uint32_t bits = __funnelshift_r(lo, hi, (uint32_t)(j & 31));
+            const uint32_t keep = len >= 32 ? 0xffffffffu : ((1u << len) - 1u);
+            word |= (bits & keep) << (e - e0);
+            e += len;
+            j = 0;
+            ++a;
         }
         tmask[i] = word;
     }
