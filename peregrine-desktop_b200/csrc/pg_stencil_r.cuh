@@ -53,7 +53,7 @@ __device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
 // Controls of a plane in group order: entry = control | kGroupFirst on the
 // first control of a group.
 constexpr uint16_t kGroupFirst = 0x8000u;
-constexpr int kRMaxWindow = 2048;  // window cells per block
+static_assert(kRMaxWindowHost == 4 * 512, "window cells per block: 4 per thread, 512 threads");
 
 // Threads per block at most and the minimum resident blocks for KR window
 // cells per thread: 16 KR corner registers per thread, so KR = 2 keeps 64
