@@ -1,0 +1,48 @@
+"""bench.py's host-side helpers, no GPU: the tiling it reports matches the
+library's register-resident tiling rule, the on-chip roofline model is the
+one stated in its docstring, and the committed ncu summary it reads the
+issue-roofline instruction count and DRAM traffic from exists and parses."""
+import importlib.util
+import os
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def bench():
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.mark.parametrize("n1,n2,rows", [(48, 48, 16), (24, 24, 24), (96, 96, 16), (12, 12, 12)])
+def test_tile_rows_follow_the_library_rule(bench, n1, n2, rows):
+    # (rows + 3) * n2 window cells: within 1024 when the 3 extra rows cost at
+    # most a quarter, else within 2048; tiles balanced over the plane
+    assert bench.blend_tile_rows(n1, n2) == rows
+    assert (rows + 3) * n2 <= 2048
+
+
+def test_onchip_model(bench):
+    class Grid:
+        n = (48, 48, 32, 15, 15, 15)
+
+    class Pr:
+        grid = Grid()
+
+    out = bench.onchip_rooflines(Pr(), 1.0e11, 4, None)
+    win = 19 / 16
+    assert out["tile_rows"] == 16
+    assert abs(out["bytes_per_update"] - (4 * win + 32 + 4 / 32)) < 1e-12
+    assert abs(out["flops_per_update"] - (2 * (16 * win + 3) + 4)) < 1e-12
+
+
+def test_committed_profile_feeds_the_rooflines(bench):
+    assert os.path.exists(bench.PROFILE_TRAFFIC)
+    wipu = bench.profiled_value("warp_instructions_per_update")
+    traffic = bench.profiled_traffic()
+    assert wipu is not None and 1.0 < wipu < 10.0
+    assert traffic is not None and traffic > 2 * 4 * 248_832_000  # at least V in and out
