@@ -161,3 +161,14 @@ def test_library_refuses_bad_arguments_without_a_gpu():
     dl = np.zeros(4, dtype=np.float32)
     assert lib.pg_adjoint(None, dl.ctypes.data, 0, 10, 1e-6, grad.ctypes.data,
                           C.byref(res)) == _lib.PG_EINVAL
+
+
+def test_binding_constants_match_the_header():
+    """The ctypes binding's kernel and storage selectors are the header's."""
+    from peregrine_hjb import _lib
+    hdr = open(os.path.join(ROOT, "include", "peregrine_hjb.h")).read()
+    defs = {k: int(v) for k, v in re.findall(r"^#define\s+(PG_(?:KERNEL|STORE)_\w+)\s+(-?\d+)", hdr, re.M)}
+    for name, value in defs.items():
+        if name.startswith("PG_KERNEL_"):
+            assert getattr(_lib, "KERNEL_" + name[len("PG_KERNEL_"):]) == value, name
+    assert _lib.STORE_Q16 == defs["PG_STORE_Q16"]
