@@ -307,6 +307,33 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device,
 int pg_measure_peaks(int device, double* smem_gbs, double* l2_gbs,
                      double* fma_tflops);
 
+/* ------------------------------------------------------------------ */
+/* self-test probes: the device's own implementations of the           */
+/* reference's functions, evaluated on caller-given inputs (host       */
+/* buffers).  The reference's self-test calls the same functions       */
+/* directly (solver/src/SelfTest.jl:208-258, 407-564); on this library */
+/* they exist only on the device, so these entry points expose them.   */
+/* ------------------------------------------------------------------ */
+
+/* step_state (rk2 = 0) or step_state_rk2 (PeregrineSolver.jl:203-279) of n
+ * states (x, y, h, vx, vy, w; body-frame velocity) under held commands
+ * (u1, u2, u3) for dt[i] in nsub[i] substeps; a diverged state comes back as
+ * NaN in every component (the reference's NANSTATE). */
+int pg_probe_step(int device, const pg_model* m, int32_t rk2, const float* states,
+                  const float* controls, const float* dt, const int32_t* nsub, int64_t n,
+                  float* out_states);
+
+/* traction_gain (PeregrineSolver.jl:126-136) of n commands. */
+int pg_probe_traction_gain(int device, const float* controls, float knee, int64_t n,
+                           float* gain);
+
+/* interp (kuhn = 0; PeregrineSolver.jl:399-466) or interp_kuhn (kuhn = 1;
+ * 571-665) of the context's current V at n states (field-frame velocity),
+ * with the given cap, nearest and vclamp flags; grads (may be NULL) gets the
+ * Kuhn gradient, 6 per state. */
+int pg_probe_interp(pg_ctx* ctx, const float* states, int64_t n, int32_t kuhn, int32_t nearest,
+                    int32_t vclamp, float cap, float* values, float* grads);
+
 /* One Jacobi sweep that allocates nothing.  No counterpart in the reference:
  * it is for callers that cannot call cudaMalloc (a host that owns all device
  * memory through its own pool or a fixed budget, or code that must not
@@ -328,8 +355,11 @@ int pg_measure_peaks(int device, double* smem_gbs, double* l2_gbs,
  * more than 8,388,608 cells are refused with PG_EINVAL.  Every call shares
  * the array and it keeps the last call's contents: each call clears or
  * writes every slot it reads, and calls that overlap on the GPU race on it.
- * The first call on a device looks up the array's device address (set-up,
- * with that device current); make that first call before any stream capture.
+ * The first call in a CUDA context looks up the array's device address in
+ * that context (set-up, with the device current); each context gets its own
+ * copy of the array.  The call is synchronous -- it copies the two totals to
+ * the host and waits for `stream` -- so it must not be called on a stream
+ * that is being captured into a CUDA graph.
  * Calls no cudaMalloc, cudaFree or other allocating routine. */
 int pg_sweep_noalloc(const pg_grid6* g, const pg_model* m, const pg_params* p,
                      const uint8_t* occ_dev, const float* ctl_dev, int32_t nctl,

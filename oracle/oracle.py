@@ -78,6 +78,8 @@ def lib() -> C.CDLL:
     L.og_sweep_inplace.restype = f64
     L.og_sweep_inplace.argtypes = [vp, vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams), i32,
                                    C.c_int]
+    L.og_cell_lookaheads.argtypes = [vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams), vp, i64,
+                                     C.c_int, vp]
     L.og_sweep_escape_jacobi.argtypes = [vp, vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams),
                                          i32, C.c_int, P(f64)]
     L.og_solve_value.restype = C.c_int
@@ -173,6 +175,19 @@ def sweep_jacobi(V, occ, g, m, ctl, p, phase=0, lo=0, hi=None, threads=0, argmin
                           ctl.size // 3, C.byref(p), phase, lo, hi, threads, C.byref(tot),
                           C.byref(mx), _p(am))
     return out, tot.value, mx.value, am
+
+
+def cell_lookaheads(V, occ, g, m, ctl, p, cells, threads=0):
+    """Every control's lookahead value for the listed cells, [len(cells), nctl]."""
+    V = np.ascontiguousarray(V, np.float32)
+    ctl = np.ascontiguousarray(ctl, np.float32)
+    cells = np.ascontiguousarray(cells, np.int64)
+    nctl = ctl.size // 3
+    out = np.empty((cells.size, nctl), np.float32)
+    lib().og_cell_lookaheads(_p(V), _p(np.ascontiguousarray(occ, np.uint8)), C.byref(g),
+                             C.byref(m), _p(ctl), nctl, C.byref(p), _p(cells), cells.size,
+                             threads, _p(out))
+    return out
 
 
 def sweep_escape_jacobi(V, occ, g, m, ctl, p, phase=0, threads=0):

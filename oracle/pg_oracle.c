@@ -689,6 +689,43 @@ void og_sweep_jacobi(const float* Vin, float* Vout, const uint8_t* occ, int8_t* 
     if (maxd) *maxd = mx;
 }
 
+void og_cell_lookaheads(const float* V, const uint8_t* occ, const og_grid* g,
+                        const og_model* m, const float* ctl, int32_t nctl,
+                        const og_params* p, const int64_t* cells, int64_t n, int threads,
+                        float* out) {
+#ifdef _OPENMP
+    int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt)
+#endif
+    for (int64_t c = 0; c < n; ++c) {
+        int64_t idx = cells[c];
+        float* o = out + c * nctl;
+        int32_t i[6];
+        unflatten(g, idx, i);
+        if (occ[((int64_t)i[0] * g->n[1] + i[1]) * g->n[2] + i[2]]) {
+            for (int32_t k = 0; k < nctl; ++k) o[k] = p->cap;
+            continue;
+        }
+        vview vv = {V, occ, (int64_t)g->n[3] * g->n[4] * g->n[5], p->cap, 0, 0};
+        og_state s;
+        s.x = axisvalue(g, 0, i[0]);
+        s.y = axisvalue(g, 1, i[1]);
+        s.h = axisvalue(g, 2, i[2]);
+        float vfx = axisvalue(g, 3, i[3]);
+        float vfy = axisvalue(g, 4, i[4]);
+        s.w = axisvalue(g, 5, i[5]);
+        float sh0, ch0;
+        og_sincos(s.h, &sh0, &ch0);
+        s.vx = ch0 * vfx + sh0 * vfy;
+        s.vy = (-sh0) * vfx + ch0 * vfy;
+        float tau0 = og_cfl_tau(g, m, vfx, vfy, s.w, p);
+        int32_t ns0 = og_substeps_for(tau0, p);
+        for (int32_t k = 0; k < nctl; ++k)
+            o[k] = lookahead_v(&vv, occ, 0, g, m, s, ctl[k], ctl[k + nctl], ctl[k + 2 * nctl],
+                               tau0, ns0, p);
+    }
+}
+
 double og_sweep_inplace(float* V, const uint8_t* occ, int8_t* pol, const og_grid* g,
                         const og_model* m, const float* ctl, int32_t nctl,
                         const og_params* p, int32_t phase, int rev) {

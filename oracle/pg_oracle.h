@@ -87,6 +87,15 @@ void og_sweep_jacobi(const float* Vin, float* Vout, const uint8_t* occ, int8_t* 
                      int32_t nctl, const og_params* p, int32_t phase, int64_t lo,
                      int64_t hi, int threads, double* total, double* maxd,
                      int16_t* argmin);
+/* Every control's lookahead value (coast first, then the table in order, as
+ * the plain scheme's cell_update scans them, PeregrineSolver.jl:1246-1275)
+ * for the n listed cells: out[i*nctl + k].  Blocked cells get cap for every
+ * control.  Plain scheme only (one horizon, no warm start, no pattern
+ * search); used to tell tied argmins from decided ones. */
+void og_cell_lookaheads(const float* V, const uint8_t* occ, const og_grid* g,
+                        const og_model* m, const float* ctl, int32_t nctl,
+                        const og_params* p, const int64_t* cells, int64_t n, int threads,
+                        float* out);
 /* The reference's own in-place sweep order (Pipeline.jl:552-568), serial so it
  * is deterministic. */
 double og_sweep_inplace(float* V, const uint8_t* occ, int8_t* pol, const og_grid* g,

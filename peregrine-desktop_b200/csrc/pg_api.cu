@@ -462,8 +462,8 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     for (int k = 0; k < 6; ++k)
         if (!(g->step[k] > 0.0f) || !std::isfinite(g->lo[k]))
             return fail(PG_EINVAL, "grid steps must be positive and origins finite");
-    if (nctl < 2 || nctl > 32767)
-        return fail(PG_EINVAL, "the control table needs coast plus at least one command");
+    if (nctl < 2) return fail(PG_EINVAL, "the control table needs coast plus at least one command");
+    if (nctl > 32767) return fail(PG_EINVAL, "the control table holds at most 32767 controls");
     if (elem_bytes(storage) == 0) return fail(PG_EINVAL, "unknown storage");
     if (storage == PG_STORE_Q16 && !(p->cap < 32.0f))
         return fail(PG_EUNSUPPORTED, "Q16 storage holds values below 32 s; value_cap is larger");
@@ -1473,6 +1473,91 @@ int pg_batch_table(pg_batch* b, int32_t table, int32_t* sweeps, double* last_max
 int pg_launch_count(pg_ctx* ctx, int64_t* launches) {
     if (!ctx || !launches) return fail(PG_EINVAL, "null argument");
     *launches = ctx->launches;
+    return PG_OK;
+}
+
+}  // extern "C"
+
+// ---- self-test probes ------------------------------------------------------
+
+namespace {
+// Device copies of a probe's host inputs and its output, freed on scope exit.
+struct ProbeBufs {
+    std::vector<void*> ptrs;
+    ~ProbeBufs() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T> cudaError_t put(T** d, const T* h, int64_t n) {
+        cudaError_t e = cudaMalloc((void**)d, (size_t)std::max<int64_t>(n, 1) * sizeof(T));
+        if (e != cudaSuccess) return e;
+        ptrs.push_back(*d);
+        return h ? cudaMemcpy(*d, h, (size_t)n * sizeof(T), cudaMemcpyHostToDevice) : cudaSuccess;
+    }
+};
+}  // namespace
+
+extern "C" {
+
+int pg_probe_step(int device, const pg_model* m, int32_t rk2, const float* states,
+                  const float* controls, const float* dt, const int32_t* nsub, int64_t n,
+                  float* out_states) {
+    if (!m || (n > 0 && (!states || !controls || !dt || !nsub || !out_states)))
+        return fail(PG_EINVAL, "null argument");
+    if (n < 0) return fail(PG_EINVAL, "negative count");
+    for (int64_t i = 0; i < n; ++i)
+        if (nsub[i] < 1 || nsub[i] > 1 << 20) return fail(PG_EINVAL, "nsub out of range");
+    if (n == 0) return PG_OK;
+    PG_CUDA(cudaSetDevice(device));
+    ProbeBufs b;
+    float *s_d, *u_d, *dt_d, *o_d;
+    int32_t* ns_d;
+    PG_CUDA(b.put(&s_d, states, 6 * n));
+    PG_CUDA(b.put(&u_d, controls, 3 * n));
+    PG_CUDA(b.put(&dt_d, dt, n));
+    PG_CUDA(b.put(&ns_d, nsub, n));
+    PG_CUDA(b.put<float>(&o_d, nullptr, 6 * n));
+    PG_CUDA(pg::launch_probe_step(*m, rk2, s_d, u_d, dt_d, ns_d, n, o_d, 0));
+    PG_CUDA(cudaMemcpy(out_states, o_d, (size_t)6 * n * sizeof(float), cudaMemcpyDeviceToHost));
+    return PG_OK;
+}
+
+int pg_probe_traction_gain(int device, const float* controls, float knee, int64_t n,
+                           float* gain) {
+    if (n > 0 && (!controls || !gain)) return fail(PG_EINVAL, "null argument");
+    if (n < 0) return fail(PG_EINVAL, "negative count");
+    if (n == 0) return PG_OK;
+    PG_CUDA(cudaSetDevice(device));
+    ProbeBufs b;
+    float *u_d, *o_d;
+    PG_CUDA(b.put(&u_d, controls, 3 * n));
+    PG_CUDA(b.put<float>(&o_d, nullptr, n));
+    PG_CUDA(pg::launch_probe_gain(u_d, knee, n, o_d, 0));
+    PG_CUDA(cudaMemcpy(gain, o_d, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost));
+    return PG_OK;
+}
+
+int pg_probe_interp(pg_ctx* ctx, const float* states, int64_t n, int32_t kuhn, int32_t nearest,
+                    int32_t vclamp, float cap, float* values, float* grads) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (n > 0 && (!states || !values)) return fail(PG_EINVAL, "null argument");
+    if (n < 0) return fail(PG_EINVAL, "negative count");
+    if (ctx->storage == PG_STORE_F64)
+        return fail(PG_EUNSUPPORTED, "the interpolation probe reads FP32 or 16-bit storage");
+    if (n == 0) return PG_OK;
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    ProbeBufs b;
+    float *s_d, *o_d, *g_d = nullptr;
+    PG_CUDA(b.put(&s_d, states, 6 * n));
+    PG_CUDA(b.put<float>(&o_d, nullptr, n));
+    if (grads) PG_CUDA(b.put<float>(&g_d, nullptr, 6 * n));
+    PG_CUDA(pg::launch_probe_interp(ctx->storage, ctx->V[ctx->cur], ctx->kp, s_d, n, kuhn,
+                                    nearest, vclamp, cap, o_d, g_d, ctx->stream));
+    ctx->launches += 1;
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    PG_CUDA(cudaMemcpy(values, o_d, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (grads)
+        PG_CUDA(cudaMemcpy(grads, g_d, (size_t)6 * n * sizeof(float), cudaMemcpyDeviceToHost));
     return PG_OK;
 }
 

@@ -26,6 +26,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "pg_device.cuh"
@@ -282,10 +283,11 @@ __device__ __forceinline__ void cmpx(T& ta, int32_t& ka, T& tb, int32_t& kb) {
     }
 }
 
-// interp_kuhn (PeregrineSolver.jl:571-665), value only
+// interp_kuhn (PeregrineSolver.jl:571-665): the value, and, when grad is
+// given, the simplex gradient along each axis (the self-test probe reads it)
 template <typename T, typename S>
 __device__ T interp_kuhn(const VView<T, S>& vv, const GridT<T>& g, const State6<T>& s, T cap,
-                         bool vclamp) {
+                         bool vclamp, T* grad = nullptr) {
     typedef Ar<T> R;
     T f1 = R::div(R::sub(s.x, g.lo[0]), g.step[0]);
     T f2 = R::div(R::sub(s.y, g.lo[1]), g.step[1]);
@@ -331,6 +333,7 @@ __device__ T interp_kuhn(const VView<T, S>& vv, const GridT<T>& g, const State6<
     const int32_t ks[6] = {k0, k1, k2, k3, k4, k5};
     T v0 = vv.get(idx[0], idx[1], idx[2], idx[3], idx[4], idx[5]);
     T acc = R::mul(R::sub((T)1, ts[0]), v0);
+    T prev = v0;
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
         const int32_t k = ks[q];
@@ -339,6 +342,9 @@ __device__ T interp_kuhn(const VView<T, S>& vv, const GridT<T>& g, const State6<
         T v = vv.get(idx[0], idx[1], idx[2], idx[3], idx[4], idx[5]);
         T wq = q < 5 ? R::sub(ts[q], ts[q + 1]) : ts[5];
         acc = R::add(acc, R::mul(wq, v));
+        // the edge walked along axis k: its difference over the axis step
+        if (grad) grad[k - 1] = R::div(R::sub(v, prev), g.step[k - 1]);
+        prev = v;
     }
     return jmin(acc, cap);
 }
@@ -784,13 +790,13 @@ static cudaError_t stencil_t(const void* Vin, void* Vout, const uint8_t* occ, co
     const int64_t blocks = stencil_blocks(kp);
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const size_t smem = stencil_smem_bytes<T, EXACT>(kp.nctl, kp.nsub, kp.nchk);
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (!(attr_set & attr_bit)) {
+    if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil<S, T, EXACT, NSUB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= attr_bit;
+        attr_set.fetch_or(attr_bit);
     }
     k_stencil<S, T, EXACT, NSUB><<<(unsigned)blocks, kp.block, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, kp, ctl, order, sb.part_sum, sb.part_max, argmin);
@@ -833,13 +839,13 @@ cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const flo
     const int coltab = kp.g.n[1] <= 255 && kp.nchk <= 4 && smem + tab <= 200 * 1024;
     if (coltab) smem += tab;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (!(attr_set & attr_bit)) {
+    if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_prep,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= attr_bit;
+        attr_set.fetch_or(attr_bit);
     }
     if (kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
     k_stencil_prep<<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask, recs, coltab);
@@ -864,13 +870,13 @@ static cudaError_t stencil_u_t(const void* Vin, void* Vout, const uint8_t* occ,
     const int64_t blocks = kp.nplanes * kp.utiles_x;
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const size_t smem = stencil_u_smem(kp.nctl);
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (!(attr_set & attr_bit)) {
+    if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_u<S, kURX, R, ARGMIN>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= attr_bit;
+        attr_set.fetch_or(attr_bit);
     }
     k_stencil_u<S, kURX, R, ARGMIN><<<(unsigned)blocks, kp.ublock, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, mask, recs, ku, order, sb.part_sum, sb.part_max, argmin);
@@ -902,13 +908,13 @@ static cudaError_t stencil_b_v(const void* Vin, void* Vout, const uint8_t* occ,
                                const uint32_t* mask, const uint32_t* recs, const KParams& kb,
                                const int32_t* order, const SweepBufs& sb, int16_t* argmin,
                                int64_t blocks, int threads, size_t smem, cudaStream_t st) {
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (!(attr_set & attr_bit)) {
+    if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_b<S, ARGMIN, VEC, OFF32>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= attr_bit;
+        attr_set.fetch_or(attr_bit);
     }
     k_stencil_b<S, ARGMIN, VEC, OFF32><<<(unsigned)blocks, threads, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, mask, recs, kb, order, sb.part_sum, sb.part_max, argmin);
@@ -968,9 +974,9 @@ cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab
                                    bool any_vec, bool any_scalar, bool off32, cudaStream_t st) {
 #define PG_BB(S)                                                                                 \
     {                                                                                            \
-        static uint64_t attr_set = 0;                                                            \
+        static std::atomic<uint64_t> attr_set{0};                                                            \
         const uint64_t attr_bit = device_bit();                                                  \
-        if (!(attr_set & attr_bit)) {                                                                         \
+        if (!(attr_set.load() & attr_bit)) {                                                                         \
             cudaError_t e = cudaSuccess;                                                         \
             void (*fns[4])(const BatchTable*, int, int64_t, int64_t, int, const int32_t*,        \
                            double*, double*) = {k_stencil_b_batch<S, true, true>,                \
@@ -981,7 +987,7 @@ cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab
                 e = cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                          200 * 1024);                                            \
             if (e != cudaSuccess) return e;                                                      \
-            attr_set |= attr_bit;                                                                     \
+            attr_set.fetch_or(attr_bit);                                                                     \
         }                                                                                        \
         if (any_vec) {                                                                           \
             if (off32)                                                                           \
@@ -1042,12 +1048,12 @@ int batch_blocks_per_sm(int storage, size_t smem, int threads) {
 
 template <typename S>
 static cudaError_t r_batch_attr() {
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (attr_set & attr_bit) return cudaSuccess;
+    if (attr_set.load() & attr_bit) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_stencil_r_batch<S, kRCellsPerThread>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    if (e == cudaSuccess) attr_set |= attr_bit;
+    if (e == cudaSuccess) attr_set.fetch_or(attr_bit);
     return e;
 }
 
@@ -1101,13 +1107,13 @@ cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const 
     const size_t smem = stencil_group_smem(kp.nctl);
     if (smem > 200 * 1024 || kp.nplanes > 0x7fffffffLL || kp.nctl > 0x7fff)
         return cudaErrorInvalidValue;
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (!(attr_set & attr_bit)) {
+    if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_group,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= attr_bit;
+        attr_set.fetch_or(attr_bit);
     }
     k_stencil_group<<<(unsigned)kp.nplanes, 128, smem, st>>>(recs, kp, order, gord);
     *launches += 1;
@@ -1131,13 +1137,13 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const size_t smem = stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, KR);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (!(attr_set & attr_bit)) {
+    if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_r<S, ARGMIN, KR>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= attr_bit;
+        attr_set.fetch_or(attr_bit);
     }
     k_stencil_r<S, ARGMIN, KR><<<(unsigned)blocks, kp.rblock, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, recs, tmask, rrow, rcol, kr, gord, sb.part_sum, sb.part_max,
@@ -1256,13 +1262,13 @@ cudaError_t launch_adj_grad(const float* V, const double* lam, const int16_t* po
                             const float* ctl, double* grad, cudaStream_t st) {
     const size_t smem = adj_grad_smem(kp.nctl);
     if (smem > 200 * 1024 || kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
-    static uint64_t attr_set = 0;
+    static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
-    if (!(attr_set & attr_bit)) {
+    if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_adj_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set |= attr_bit;
+        attr_set.fetch_or(attr_bit);
     }
     k_adj_grad<<<(unsigned)kp.nplanes, 128, smem, st>>>(V, lam, pol, active, recs, kp, ctl, grad);
     return cudaGetLastError();
@@ -1286,6 +1292,94 @@ cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t
         case PG_STORE_BF16: k_encode<__nv_bfloat16><<<b, 256, 0, st>>>((const __nv_bfloat16*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
         case PG_STORE_Q16: k_encode<Q16><<<b, 256, 0, st>>>((const Q16*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
         case PG_STORE_F64: k_encode<double><<<b, 256, 0, st>>>((const double*)V, kp, dtype, scale, escape_scale, lo, n, out, counts); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Self-test probes: the device's own implementations of the reference's
+// functions evaluated on given inputs, so the self-test can check what the
+// sweeps compute (SelfTest.jl:208-258, 407-564 call the same functions).
+// ---------------------------------------------------------------------------
+
+// step_state / step_state_rk2 (PeregrineSolver.jl:203-279): one integration
+// per item; a diverged state comes back as NaN in every component, as the
+// reference's NANSTATE.
+__global__ void k_probe_step(pg_model mdl, int32_t rk2, const float* __restrict__ states,
+                             const float* __restrict__ controls, const float* __restrict__ dt,
+                             const int32_t* __restrict__ nsub, int64_t n,
+                             float* __restrict__ out) {
+    ModelT<float> m;
+    load_model(m, mdl);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float* si = states + 6 * i;
+        State6<float> s{si[0], si[1], si[2], si[3], si[4], si[5]};
+        const bool ok = integrate(m, s, controls[3 * i], controls[3 * i + 1], controls[3 * i + 2],
+                                  dt[i], nsub[i], rk2 != 0, (float*)nullptr, (float*)nullptr);
+        const float nanv = __int_as_float(0x7fc00000);
+        float* o = out + 6 * i;
+        o[0] = ok ? s.x : nanv; o[1] = ok ? s.y : nanv; o[2] = ok ? s.h : nanv;
+        o[3] = ok ? s.vx : nanv; o[4] = ok ? s.vy : nanv; o[5] = ok ? s.w : nanv;
+    }
+}
+
+// traction_gain (PeregrineSolver.jl:126-136)
+__global__ void k_probe_gain(const float* __restrict__ controls, float knee, int64_t n,
+                             float* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = traction_gain(controls[3 * i], controls[3 * i + 1], controls[3 * i + 2], knee);
+}
+
+// interp / interp_kuhn (PeregrineSolver.jl:399-466, 571-665) of the stored V
+// at given states; grads (6 per state) for the Kuhn form when non-null.
+template <typename S>
+__global__ void k_probe_interp(const S* __restrict__ V, KParams kp, const float* __restrict__ states,
+                               int64_t n, int32_t kuhn, int32_t nearest, int32_t vclamp, float cap,
+                               float* __restrict__ out, float* __restrict__ grads) {
+    GridT<float> g;
+    load_grid(g, kp.g);
+    VView<float, S> vv{V, nullptr, make_layout(kp), cap, false, true};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float* si = states + 6 * i;
+        State6<float> s{si[0], si[1], si[2], si[3], si[4], si[5]};
+        if (kuhn) {
+            float gr[6] = {0, 0, 0, 0, 0, 0};
+            out[i] = interp_kuhn(vv, g, s, cap, vclamp != 0, gr);
+            if (grads)
+                for (int k = 0; k < 6; ++k) grads[6 * i + k] = gr[k];
+        } else {
+            out[i] = interp_ml(vv, g, s, nearest != 0, cap, vclamp != 0);
+        }
+    }
+}
+
+cudaError_t launch_probe_step(const pg_model& m, int32_t rk2, const float* states,
+                              const float* controls, const float* dt, const int32_t* nsub,
+                              int64_t n, float* out, cudaStream_t st) {
+    k_probe_step<<<grid_for(n, 128), 128, 0, st>>>(m, rk2, states, controls, dt, nsub, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probe_gain(const float* controls, float knee, int64_t n, float* out,
+                              cudaStream_t st) {
+    k_probe_gain<<<grid_for(n, 128), 128, 0, st>>>(controls, knee, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probe_interp(int storage, const void* V, const KParams& kp, const float* states,
+                                int64_t n, int32_t kuhn, int32_t nearest, int32_t vclamp,
+                                float cap, float* out, float* grads, cudaStream_t st) {
+    const int b = grid_for(n, 128);
+    switch (storage) {
+        case PG_STORE_F32: k_probe_interp<float><<<b, 128, 0, st>>>((const float*)V, kp, states, n, kuhn, nearest, vclamp, cap, out, grads); break;
+        case PG_STORE_F16: k_probe_interp<__half><<<b, 128, 0, st>>>((const __half*)V, kp, states, n, kuhn, nearest, vclamp, cap, out, grads); break;
+        case PG_STORE_BF16: k_probe_interp<__nv_bfloat16><<<b, 128, 0, st>>>((const __nv_bfloat16*)V, kp, states, n, kuhn, nearest, vclamp, cap, out, grads); break;
+        case PG_STORE_Q16: k_probe_interp<Q16><<<b, 128, 0, st>>>((const Q16*)V, kp, states, n, kuhn, nearest, vclamp, cap, out, grads); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

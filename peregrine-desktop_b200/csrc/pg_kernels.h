@@ -90,6 +90,15 @@ size_t stencil_u_smem_bytes(const KParams& kp);
 size_t stencil_recs_bytes(const KParams& kp);
 size_t stencil_mask_bytes(const KParams& kp);
 
+cudaError_t launch_probe_step(const pg_model& m, int32_t rk2, const float* states,
+                              const float* controls, const float* dt, const int32_t* nsub,
+                              int64_t n, float* out, cudaStream_t st);
+cudaError_t launch_probe_gain(const float* controls, float knee, int64_t n, float* out,
+                              cudaStream_t st);
+cudaError_t launch_probe_interp(int storage, const void* V, const KParams& kp, const float* states,
+                                int64_t n, int32_t kuhn, int32_t nearest, int32_t vclamp,
+                                float cap, float* out, float* grads, cudaStream_t st);
+
 int64_t cellform_blocks(int64_t ncells);
 int64_t stencil_blocks(const KParams& kp);
 size_t stencil_smem(int storage, bool exact, const KParams& kp);

@@ -17,13 +17,18 @@
 // shares it and it keeps the last call's contents; each call writes every
 // slot it reads before reading it and clears the two totals first.  Calls
 // that overlap on the GPU (on different streams, or from different host
-// threads) race on it.
+// threads) race on it.  The call is synchronous: it reads the two totals
+// back and waits for its stream, so it must not be issued on a stream that
+// is being captured into a CUDA graph.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "pg_kernels.h"
 #include "pg_types.h"
@@ -41,30 +46,57 @@ constexpr int64_t kMaxCells = kMaxParts * pg::kCellThreads;
 // variable; it is never a device address there.
 static __device__ __align__(256) double g_sweep_scratch[2 * kMaxParts + 2];
 
-// The array's device address on each device, looked up on the first call
-// made with that device current.
-constexpr int kMaxDevices = 64;
+// The array's device address in each CUDA context, looked up on the first
+// call made with that context current.  The module holding the array is
+// loaded once per context, so a caller that makes its own driver-API context
+// current (cuCtxCreate) gets that context's copy, not the primary context's.
+// The current context is read through the driver entry point the runtime
+// hands out, so the library does not link libcuda itself.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
 std::mutex g_scratch_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
+std::vector<std::pair<CUcontext, double*>> g_scratch_ptr;
+
+// The context current on this thread (null when none is yet).
+int current_context(CUcontext* ctx) {
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !f)
+            return pg::set_last_error(PG_ECUDA, "cuCtxGetCurrent is not available from the driver");
+        fn = reinterpret_cast<CtxGetCurrentFn>(f);
+    }
+    *ctx = nullptr;
+    if (fn(ctx) != CUDA_SUCCESS)
+        return pg::set_last_error(PG_ECUDA, "cuCtxGetCurrent failed");
+    return PG_OK;
+}
 
 int scratch_on_current_device(double** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-        return pg::set_last_error(PG_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices)
-        return pg::set_last_error(PG_EUNSUPPORTED, "device index beyond 63");
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        double* p = nullptr;
-        e = cudaGetSymbolAddress((void**)&p, g_sweep_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return pg::set_last_error(
-                PG_ECUDA, std::string("cudaGetSymbolAddress(sweep scratch): ") +
-                              cudaGetErrorString(e));
-        g_scratch_ptr[dev] = p;
+    CUcontext cx = nullptr;
+    int rc = current_context(&cx);
+    if (rc) return rc;
+    for (const auto& kv : g_scratch_ptr)
+        if (cx && kv.first == cx) {
+            *out = kv.second;
+            return PG_OK;
+        }
+    // set-up: the array's address in the current context (the runtime makes
+    // the current device's primary context current when no context is)
+    double* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_sweep_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return pg::set_last_error(PG_ECUDA, std::string("cudaGetSymbolAddress(sweep scratch): ") +
+                                                cudaGetErrorString(e));
+    if (!cx) {
+        rc = current_context(&cx);
+        if (rc) return rc;
+        if (!cx) return pg::set_last_error(PG_ECUDA, "no current CUDA context after set-up");
     }
-    *out = g_scratch_ptr[dev];
+    g_scratch_ptr.emplace_back(cx, p);
+    *out = p;
     return PG_OK;
 }
 
@@ -94,8 +126,9 @@ int pg_sweep_noalloc(const pg_grid6* g, const pg_model* m, const pg_params* p,
             PG_EINVAL, "pg_sweep_noalloc takes grids of at most 8388608 cells (its fixed working "
                        "array holds 65536 block partials); use pg_load_problem/pg_sweep for "
                        "larger grids");
-    if (nctl < 2 || nctl > 32767)
+    if (nctl < 2)
         return set_last_error(PG_EINVAL, "the control table needs coast plus at least one command");
+    if (nctl > 32767) return set_last_error(PG_EINVAL, "the control table holds at most 32767 controls");
     if (!(p->cap > 0.0f)) return set_last_error(PG_EINVAL, "value_cap must be positive");
     if (p->nsub < 1) return set_last_error(PG_EINVAL, "substeps must be >= 1");
     if (p->checks < 1) return set_last_error(PG_EINVAL, "sweep_checks must be >= 1");

@@ -35,7 +35,7 @@ EXPORTS = (
     "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
     "pg_launch_count", "pg_set_tile_rows", "pg_batch_create", "pg_batch_destroy",
     "pg_batch_add", "pg_batch_solve", "pg_batch_table", "pg_adjoint", "pg_measure_peaks",
-    "pg_sweep_noalloc",
+    "pg_sweep_noalloc", "pg_probe_step", "pg_probe_traction_gain", "pg_probe_interp",
 )
 
 
@@ -140,6 +140,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "pg_measure_peaks": (C.c_int, [C.c_int, P(f64), P(f64), P(f64)]),
         "pg_sweep_noalloc": (C.c_int, [P(Grid6), P(Model), P(Params), vp, vp, i32, vp, vp, i32,
                                        vp, P(f64), P(f64)]),
+        "pg_probe_step": (C.c_int, [C.c_int, P(Model), i32, vp, vp, vp, vp, i64, vp]),
+        "pg_probe_traction_gain": (C.c_int, [C.c_int, vp, C.c_float, i64, vp]),
+        "pg_probe_interp": (C.c_int, [vp, vp, i64, i32, i32, i32, C.c_float, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -215,6 +218,7 @@ class Context:
                                          int(storage)))
         self.ncells = int(np.prod(np.array(n, dtype=np.int64)))
         self.nctl = nctl
+        self._cap = float(params.cap)
         self._keep = (occ, ctl)
 
     def solve(self, tidx: np.ndarray, iters: int, tol: float, opts: SolveOpts | None = None,
@@ -297,6 +301,43 @@ class Context:
         n = C.c_int64()
         _check(self._lib.pg_launch_count(self._h, C.byref(n)))
         return n.value
+
+    def probe_interp(self, states, kuhn=False, nearest=False, vclamp=False, cap=None,
+                     grads=False):
+        """interp / interp_kuhn of the current V at states [n, 6] (field-frame
+        velocity) on the device; returns values (and [n, 6] Kuhn gradients)."""
+        st = np.ascontiguousarray(np.asarray(states, np.float32).reshape(-1, 6))
+        n = st.shape[0]
+        out = np.empty(n, np.float32)
+        gr = np.empty((n, 6), np.float32) if grads else None
+        cap = float(self._cap if cap is None else cap)
+        _check(self._lib.pg_probe_interp(self._h, _ptr(st), n, int(kuhn), int(nearest),
+                                         int(vclamp), cap, _ptr(out), _ptr(gr)))
+        return (out, gr) if grads else out
+
+
+def probe_step(model: Model, states, controls, dt, nsub, rk2=True, device: int = 0):
+    """step_state / step_state_rk2 on the device for states [n, 6] under
+    controls [n, 3]; dt and nsub are scalars or [n]; NaN rows = diverged."""
+    lib = load_library()
+    st = np.ascontiguousarray(np.asarray(states, np.float32).reshape(-1, 6))
+    n = st.shape[0]
+    u = np.ascontiguousarray(np.broadcast_to(np.asarray(controls, np.float32).reshape(-1, 3), (n, 3)))
+    dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float32), (n,)))
+    ns = np.ascontiguousarray(np.broadcast_to(np.asarray(nsub, np.int32), (n,)))
+    out = np.empty((n, 6), np.float32)
+    _check(lib.pg_probe_step(int(device), C.byref(model), int(rk2), _ptr(st), _ptr(u), _ptr(dts),
+                             _ptr(ns), n, _ptr(out)))
+    return out
+
+
+def probe_traction_gain(controls, knee, device: int = 0):
+    """traction_gain on the device for controls [n, 3]."""
+    lib = load_library()
+    u = np.ascontiguousarray(np.asarray(controls, np.float32).reshape(-1, 3))
+    out = np.empty(u.shape[0], np.float32)
+    _check(lib.pg_probe_traction_gain(int(device), _ptr(u), C.c_float(knee), u.shape[0], _ptr(out)))
+    return out
 
 
 def measure_peaks(device: int = 0) -> dict:
