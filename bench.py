@@ -3,11 +3,13 @@
 value-iteration sweep on one B200 per rank.
 
 A step is one Jacobi sweep over the whole table (every cell x every control).
-Workload: 48 x 48 x 32 x 15 x 15 x 15 = 248,832,000 cells, 125 controls
-({-1,-0.5,0,0.5,1}^3), dt 0.04 s, RK2, 6 rectangular obstacles, seed 0 --
-one table per GPU; with --gpus N every rank solves its own independent table
-(different seed), so per-GPU work is fixed (weak scaling, no data-path
-collective; the only collective is the max of the timings).
+Workload: 96 x 96 x 64 x 21 x 21 x 21 = 5,462,360,064 cells, 125 controls
+({-1,-0.5,0,0.5,1}^3), dt 0.03 s, RK2, 8 rectangular obstacles, seed 0 (the
+largest table that fits one B200 in core; `--workload medium` runs the
+48 x 48 x 32 x 15^3 table) -- one table per GPU; with --gpus N every rank
+solves its own independent table (different seed), so per-GPU work is fixed
+(weak scaling, no data-path collective; the only collective is the max of the
+timings).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -34,8 +36,19 @@ for _p in (ROOT, PKG):
 
 METRIC = "Bellman cell-control updates/s; time-to-converge vs plain FP32 at ≤2 ms max err"
 UNIT = "cell-control updates/s"
-WORKLOAD = "medium"
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_stencil_r_medium_fp32.md")
+WORKLOAD = "large"
+KERNEL_SOURCE = os.path.join(PKG, "csrc", "pg_stencil_r.cuh")
+
+
+def profile_path():
+    """The committed ncu summary of the sweep kernel on this workload."""
+    return os.path.join(ROOT, "profiles", f"k_stencil_r_{WORKLOAD}_fp32.md")
+
+
+def kernel_source_sha():
+    import hashlib
+    with open(KERNEL_SOURCE, "rb") as fh:
+        return hashlib.sha256(fh.read()).hexdigest()
 
 
 def peaks():
@@ -86,32 +99,46 @@ def onchip_rooflines(pr, rate_per_gpu: float, elem: int, peaks_onchip) -> dict:
     return out
 
 
+def _profile_lines():
+    p = profile_path()
+    if not os.path.exists(p):
+        return None
+    return [ln.strip() for ln in open(p)]
+
+
+def profile_current() -> bool:
+    """Whether the committed profile was captured from the kernel source this
+    tree builds (its `source_sha256:` line against pg_stencil_r.cuh)."""
+    lines = _profile_lines()
+    if not lines:
+        return False
+    for ln in lines:
+        if ln.startswith("source_sha256:"):
+            return ln.split(":", 1)[1].strip().split()[0] == kernel_source_sha()
+    return False
+
+
 def profiled_value(key: str):
     """A number from the committed ncu summary of the sweep kernel (a line
-    `key: N ...`), or None."""
-    if not os.path.exists(PROFILE_TRAFFIC):
+    `key: N ...`), or None -- also None when that profile was captured from
+    another version of the kernel source, so a stale figure is never
+    reported as this kernel's."""
+    lines = _profile_lines()
+    if not lines or not profile_current():
         return None
-    for line in open(PROFILE_TRAFFIC):
-        if line.strip().startswith(key + ":"):
+    for ln in lines:
+        if ln.startswith(key + ":"):
             try:
-                return float(line.split(":", 1)[1].strip().split()[0])
+                return float(ln.split(":", 1)[1].strip().split()[0])
             except ValueError:
                 return None
     return None
 
 
 def profiled_traffic():
-    """DRAM bytes per launch of the stencil kernel from the committed ncu
+    """DRAM bytes per launch of the sweep kernel from the committed ncu
     summary (a line `traffic_bytes_per_launch: N`), or None."""
-    if not os.path.exists(PROFILE_TRAFFIC):
-        return None
-    for line in open(PROFILE_TRAFFIC):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
+    return profiled_value("traffic_bytes_per_launch")
 
 
 class Clocks:
@@ -182,11 +209,11 @@ def cpu_sample(pr, budget_s: float, threads: int, rank_seed: int = 0):
     mid = pr.ncells // 2
     probe = 8192 * max(1, threads)
     t0 = time.perf_counter()
-    og.sweep_jacobi(V, pr.occ, g, m, pr.ctl, p, 0, mid, mid + probe, threads)
+    og.sweep_jacobi_slab(V, pr.occ, g, m, pr.ctl, p, mid, mid + probe, 0, threads)
     rate = probe / max(time.perf_counter() - t0, 1e-6)
     n = int(min(max(rate * budget_s, probe), pr.ncells // 4))
     t0 = time.perf_counter()
-    og.sweep_jacobi(V, pr.occ, g, m, pr.ctl, p, 0, mid, mid + n, threads)
+    og.sweep_jacobi_slab(V, pr.occ, g, m, pr.ctl, p, mid, mid + n, 0, threads)
     dt = time.perf_counter() - t0
     return n, dt, n * pr.nctl / dt
 
@@ -197,15 +224,19 @@ def problem_for_rank(rank: int):
 
 
 def workload_config(pr, extra=None):
+    from peregrine_hjb.synth import WORKLOADS
     n = pr.grid.n
+    rects = WORKLOADS[WORKLOAD]["rects"]
     cfg = {
         "workload": f"plain FP32 value iteration, {n[0]}x{n[1]}x{n[2]}x{n[3]}x{n[4]}x{n[5]} "
-                    f"= {pr.ncells} cells, {pr.nctl} controls (cube5), dt {pr.cfg['dt']} s, RK2, "
-                    f"6 rectangles, 64-corner multilinear, one table per GPU",
+                    f"= {pr.ncells} cells, {pr.nctl} controls ({pr.cfg['control_set']}), "
+                    f"dt {pr.cfg['dt']} s, RK2, {rects} rectangles, 64-corner multilinear, "
+                    f"one table per GPU",
         "cells": pr.ncells,
         "controls": pr.nctl,
         "step": "one Jacobi sweep over every cell and control",
-        "l2": "inputs larger than L2 (V is 0.995 GB per buffer, two buffers)",
+        "l2": f"inputs larger than L2 (V is {pr.ncells * 4 / 1e9:.3g} GB per buffer, two "
+              f"buffers)",
         "kernel": "k_stencil_r<float> (register-resident blend-then-shift)",
     }
     if extra:
@@ -292,15 +323,15 @@ def run_ours(args, rank, world, local_rank):
         return 0
 
     # ---- end to end through the public one-shot call, host buffers in/out
-    # sweeps per end-to-end call: a real solve runs hundreds; ten keep the
+    # sweeps per end-to-end call: a real solve runs hundreds; a few keep the
     # timed calls short while the per-call load, prep and copies still count
-    e2e_sweeps = 10
+    e2e_sweeps = 10 if pr.ncells < (1 << 30) else 2
     occ_h = torch.from_numpy(pr.occ).pin_memory()
     ctl_h = torch.from_numpy(pr.ctl).pin_memory()
     tidx_h = torch.from_numpy(pr.seeds).pin_memory()
     V_h = torch.empty(pr.ncells, dtype=torch.float32).pin_memory()
     occ_n, ctl_n, tidx_n, V_n = (x.numpy() for x in (occ_h, ctl_h, tidx_h, V_h))
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 3 if pr.ncells < (1 << 30) else 2))
     import ctypes as C
     lib = _lib.load_library()
     res = _lib.SolveResult()

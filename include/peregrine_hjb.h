@@ -218,6 +218,15 @@ int pg_encode(pg_ctx* ctx, int32_t dtype, double scale, double escape_scale,
 int pg_time_sweeps(pg_ctx* ctx, int32_t warmup, int32_t steps, int32_t kernel,
                    double* ms_per_sweep);
 
+/* A limit on each wait for a sweep in the solve loops (pg_solve,
+ * pg_solve_value, pg_solve_escape, pg_sweep): when the sweep and its
+ * residual copy have not finished `seconds` after the host starts waiting,
+ * the call returns PG_ETIMEOUT instead of blocking; the queued work still
+ * completes on the device, and pg_destroy waits for it.  0 (the default)
+ * waits without a limit.  The reference blocks in CUDA.synchronize after
+ * every sweep (solver/src/Gpu.jl:33-36); this bounds that wait. */
+int pg_set_wait_timeout(pg_ctx* ctx, double seconds);
+
 /* Number of this library's kernel launches since the context was created. */
 int pg_launch_count(pg_ctx* ctx, int64_t* launches);
 

@@ -78,6 +78,8 @@ def lib() -> C.CDLL:
     L.og_sweep_inplace.restype = f64
     L.og_sweep_inplace.argtypes = [vp, vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams), i32,
                                    C.c_int]
+    L.og_sweep_jacobi_slab.argtypes = [vp, vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams), i32,
+                                       i64, i64, C.c_int, P(f64), P(f64)]
     L.og_cell_lookaheads.argtypes = [vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams), vp, i64,
                                      C.c_int, vp]
     L.og_sweep_escape_jacobi.argtypes = [vp, vp, vp, P(OGrid), P(OModel), vp, i32, P(OParams),
@@ -175,6 +177,20 @@ def sweep_jacobi(V, occ, g, m, ctl, p, phase=0, lo=0, hi=None, threads=0, argmin
                           ctl.size // 3, C.byref(p), phase, lo, hi, threads, C.byref(tot),
                           C.byref(mx), _p(am))
     return out, tot.value, mx.value, am
+
+
+def sweep_jacobi_slab(V, occ, g, m, ctl, p, lo, hi, phase=0, threads=0):
+    """One Jacobi sweep of the cells [lo, hi) only: returns (V' on the slab,
+    L1 total, max-norm); V is the whole table it reads from."""
+    V = np.ascontiguousarray(V, np.float32)
+    ctl = np.ascontiguousarray(ctl, np.float32)
+    out = np.empty(hi - lo, np.float32)
+    tot = C.c_double()
+    mx = C.c_double()
+    lib().og_sweep_jacobi_slab(_p(V), _p(out), _p(np.ascontiguousarray(occ, np.uint8)), C.byref(g),
+                               C.byref(m), _p(ctl), ctl.size // 3, C.byref(p), phase, lo, hi,
+                               threads, C.byref(tot), C.byref(mx))
+    return out, tot.value, mx.value
 
 
 def cell_lookaheads(V, occ, g, m, ctl, p, cells, threads=0):

@@ -637,10 +637,13 @@ static inline int8_t qpol(float v) {
 
 #define OG_CHUNK 4096
 
-void og_sweep_jacobi(const float* Vin, float* Vout, const uint8_t* occ, int8_t* pol,
-                     const og_grid* g, const og_model* m, const float* ctl, int32_t nctl,
-                     const og_params* p, int32_t phase, int64_t lo, int64_t hi, int threads,
-                     double* total, double* maxd, int16_t* argmin) {
+/* The sweep over [lo, hi); cell idx's result goes to Vout[idx - out_off]
+ * (out_off = 0: a whole-table Vout; out_off = lo: a slab of hi - lo). */
+static void sweep_jacobi_impl(const float* Vin, float* Vout, int64_t out_off, const uint8_t* occ,
+                              int8_t* pol, const og_grid* g, const og_model* m, const float* ctl,
+                              int32_t nctl, const og_params* p, int32_t phase, int64_t lo,
+                              int64_t hi, int threads, double* total, double* maxd,
+                              int16_t* argmin) {
     int64_t n = hi - lo;
     int64_t nchunk = (n + OG_CHUNK - 1) / OG_CHUNK;
     double* part = (double*)calloc((size_t)(nchunk > 0 ? nchunk : 1), sizeof(double));
@@ -662,7 +665,7 @@ void og_sweep_jacobi(const float* Vin, float* Vout, const uint8_t* occ, int8_t* 
             int blocked = occ[xy * g->n[2] + i3] != 0;
             if (argmin) argmin[idx] = blocked ? (int16_t)-1 : ctl_index(ctl, nctl, ub);
             if (c < old) {
-                Vout[idx] = c;
+                Vout[idx - out_off] = c;
                 if (pol) {
                     pol[3 * idx] = qpol(ub[0]);
                     pol[3 * idx + 1] = qpol(ub[1]);
@@ -672,7 +675,7 @@ void og_sweep_jacobi(const float* Vin, float* Vout, const uint8_t* occ, int8_t* 
                 s += d;
                 if (d > mx) mx = d;
             } else {
-                Vout[idx] = old;
+                Vout[idx - out_off] = old;
             }
         }
         part[cidx] = s;
@@ -724,6 +727,22 @@ void og_cell_lookaheads(const float* V, const uint8_t* occ, const og_grid* g,
             o[k] = lookahead_v(&vv, occ, 0, g, m, s, ctl[k], ctl[k + nctl], ctl[k + 2 * nctl],
                                tau0, ns0, p);
     }
+}
+
+void og_sweep_jacobi(const float* Vin, float* Vout, const uint8_t* occ, int8_t* pol,
+                     const og_grid* g, const og_model* m, const float* ctl, int32_t nctl,
+                     const og_params* p, int32_t phase, int64_t lo, int64_t hi, int threads,
+                     double* total, double* maxd, int16_t* argmin) {
+    sweep_jacobi_impl(Vin, Vout, 0, occ, pol, g, m, ctl, nctl, p, phase, lo, hi, threads, total,
+                      maxd, argmin);
+}
+
+void og_sweep_jacobi_slab(const float* Vin, float* Vout_slab, const uint8_t* occ,
+                          const og_grid* g, const og_model* m, const float* ctl, int32_t nctl,
+                          const og_params* p, int32_t phase, int64_t lo, int64_t hi, int threads,
+                          double* total, double* maxd) {
+    sweep_jacobi_impl(Vin, Vout_slab, lo, occ, NULL, g, m, ctl, nctl, p, phase, lo, hi, threads,
+                      total, maxd, NULL);
 }
 
 double og_sweep_inplace(float* V, const uint8_t* occ, int8_t* pol, const og_grid* g,

@@ -96,6 +96,12 @@ void og_cell_lookaheads(const float* V, const uint8_t* occ, const og_grid* g,
                         const og_model* m, const float* ctl, int32_t nctl,
                         const og_params* p, const int64_t* cells, int64_t n, int threads,
                         float* out);
+/* og_sweep_jacobi over cells [lo, hi) writing only that slab:
+ * Vout_slab[idx - lo] (hi - lo floats); no policy, no argmin. */
+void og_sweep_jacobi_slab(const float* Vin, float* Vout_slab, const uint8_t* occ,
+                          const og_grid* g, const og_model* m, const float* ctl, int32_t nctl,
+                          const og_params* p, int32_t phase, int64_t lo, int64_t hi, int threads,
+                          double* total, double* maxd);
 /* The reference's own in-place sweep order (Pipeline.jl:552-568), serial so it
  * is deterministic. */
 double og_sweep_inplace(float* V, const uint8_t* occ, int8_t* pol, const og_grid* g,

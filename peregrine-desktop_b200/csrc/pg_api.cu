@@ -14,6 +14,7 @@
 #include <cstring>
 #include <string>
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "pg_kernels.h"
@@ -63,6 +64,8 @@ struct pg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_wait = nullptr;  // the per-sweep residual copy, for bounded waits
+    double wait_timeout_s = 0.0;    // 0: wait for each sweep without a limit
     int64_t launches = 0;
 
     bool loaded = false;
@@ -85,8 +88,6 @@ struct pg_ctx {
     bool blend_ok = false;   // the blend-then-shift tiling fits (shared memory, row width)
     bool gather_ok = false;  // the 64-corner masked gather fits its shared memory
     uint16_t* gord_d = nullptr;  // per plane, its controls in corner-group order
-    int2* rctab_d = nullptr;     // per (plane, control): its row, then column successor
-                                 // entries (rows for the current tiling)
     uint32_t* tmask_d = nullptr; // admissibility per (plane, tile, control) in tile order
     size_t tmask_cap = 0;
     bool rblend_ok = false;      // the register-resident blend can run (tables, tiling)
@@ -127,8 +128,6 @@ struct pg_ctx {
         gather_ok = false;
         if (gord_d) cudaFree(gord_d);
         gord_d = nullptr;
-        if (rctab_d) cudaFree(rctab_d);
-        rctab_d = nullptr;
         if (tmask_d) cudaFree(tmask_d);
         tmask_d = nullptr;
         tmask_cap = 0;
@@ -220,33 +219,29 @@ void r_tiling(pg::KParams& kp, int32_t rows) {
 // of shared memory per SM less 1 KB reserved per block; or,
 // with more than 256 threads, the block has the SM to itself anyway) and the
 // re-reading blend runs elsewhere.
-// The column entries follow the row entries in rctab_d.
-const int2* r_cols(const pg_ctx* ctx) {
-    return ctx->rctab_d + (size_t)ctx->kp.nplanes * ctx->kp.nctl * ctx->kp.g.n[0];
-}
-
 bool r_smem_fits(const pg::KParams& kp) {
     return kp.rtile_x > 0 &&
            pg::stencil_r_smem_bytes(kp) <= (size_t)(kp.rblock > 256 ? 200 : 110) * 1024;
 }
 
+// Planes of row-order mask words that fit a staging buffer of `bytes`.
+int64_t mask_chunk_planes(const pg::KParams& kp, size_t bytes) {
+    const size_t per = pg::stencil_mask_bytes(kp) / (size_t)kp.nplanes;
+    const int64_t c = (int64_t)(bytes / std::max<size_t>(per, 1));
+    return std::max<int64_t>(1, std::min<int64_t>(c, kp.nplanes));
+}
+
 // (Re)builds the tile-order mask of the register-resident blend for the
-// current tiling and sets rblend_ok.  The blend stays off (the re-reading
-// blend runs) when its tables or the mask do not fit in device memory with
-// 2 GiB to spare.
+// current tiling and sets rblend_ok.  From the row-order mask when the
+// context keeps it; otherwise the records and the row-order words are made
+// again by k_stencil_prep a chunk of planes at a time into a staging buffer
+// of at most 4 GiB, and each chunk regrouped before the next.  The blend
+// stays off (the re-reading blend, or the row stencil, runs) when the tile
+// mask does not fit in device memory with 2 GiB to spare.
 int build_r_tables(pg_ctx* ctx) {
     pg::KParams& kp = ctx->kp;
     ctx->rblend_ok = false;
-    if (!ctx->mask_ok || !ctx->gord_d || !ctx->rctab_d || !r_smem_fits(kp)) return PG_OK;
-    // the successor entries (their row form depends on the tiling)
-    {
-        int2* rrow = ctx->rctab_d;
-        int2* rcol = rrow + (size_t)kp.nplanes * kp.nctl * kp.g.n[0];
-        cudaError_t e = pg::launch_stencil_rc(ctx->recs_d, kp, rrow, rcol, ctx->stream,
-                                              &ctx->launches);
-        if (e != cudaSuccess)
-            return fail(PG_ECUDA, std::string("successor table: ") + cudaGetErrorString(e));
-    }
+    if (!ctx->recs_d || !ctx->gord_d || !r_smem_fits(kp)) return PG_OK;
     const size_t need = pg::stencil_tmask_bytes(kp);
     if (need > ctx->tmask_cap) {
         PG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -262,9 +257,37 @@ int build_r_tables(pg_ctx* ctx) {
         }
         ctx->tmask_cap = need;
     }
-    cudaError_t e = pg::launch_stencil_tmask(ctx->mask_d, kp, ctx->tmask_d, ctx->stream,
+    if (ctx->mask_d) {
+        cudaError_t e = pg::launch_stencil_tmask(ctx->mask_d, kp, 0, kp.nplanes, ctx->tmask_d,
+                                                 ctx->stream, &ctx->launches);
+        if (e != cudaSuccess)
+            return fail(PG_ECUDA, std::string("tile mask: ") + cudaGetErrorString(e));
+    } else {
+        size_t fr = 0, tot = 0;
+        PG_CUDA(cudaMemGetInfo(&fr, &tot));
+        const size_t spare = fr > ((size_t)2 << 30) ? fr - ((size_t)2 << 30) : 0;
+        const int64_t chunk = mask_chunk_planes(kp, std::min(spare, (size_t)4 << 30));
+        const size_t cb = pg::stencil_mask_bytes(kp) / (size_t)kp.nplanes * (size_t)chunk;
+        uint32_t* tmp = nullptr;
+        if (cb > spare || cudaMalloc(&tmp, cb) != cudaSuccess) {
+            cudaGetLastError();
+            return PG_OK;
+        }
+        cudaError_t e = cudaSuccess;
+        for (int64_t p0 = 0; p0 < kp.nplanes && e == cudaSuccess; p0 += chunk) {
+            const int64_t np = std::min<int64_t>(chunk, kp.nplanes - p0);
+            e = pg::launch_stencil_prep(ctx->occ_d, kp, ctx->ctl_d, tmp, ctx->recs_d, p0, np,
+                                        ctx->stream, &ctx->launches);
+            if (e == cudaSuccess)
+                e = pg::launch_stencil_tmask(tmp, kp, p0, np, ctx->tmask_d, ctx->stream,
                                              &ctx->launches);
-    if (e != cudaSuccess) return fail(PG_ECUDA, std::string("tile mask: ") + cudaGetErrorString(e));
+        }
+        cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+        cudaFree(tmp);
+        if (e == cudaSuccess) e = e2;
+        if (e != cudaSuccess)
+            return fail(PG_ECUDA, std::string("tile mask from chunks: ") + cudaGetErrorString(e));
+    }
     ctx->rblend_ok = true;
     return PG_OK;
 }
@@ -291,7 +314,7 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
     const void* vin = ctx->V[ctx->cur];
     void* vout = ctx->V[1 - ctx->cur];
     cudaError_t e;
-    const bool r_ok = ctx->mask_ok && ctx->rblend_ok && ctx->storage != PG_STORE_F64;
+    const bool r_ok = ctx->rblend_ok && ctx->storage != PG_STORE_F64;
     const bool b_ok = ctx->mask_ok && ctx->blend_ok && ctx->storage != PG_STORE_F64;
     if (ctx->storage == PG_STORE_Q16 &&
         (esc || !((kernel == PG_KERNEL_STENCIL && (r_ok || b_ok)) ||
@@ -306,8 +329,7 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
                                 ctx->stream, &ctx->launches);
     else if (kernel == PG_KERNEL_STENCIL && r_ok)
         e = pg::launch_stencil_r(ctx->storage, vin, vout, ctx->occ_d, ctx->recs_d, ctx->tmask_d,
-                                 ctx->rctab_d, r_cols(ctx), ctx->kp, ctx->gord_d, sb, argmin_d,
-                                 ctx->stream, &ctx->launches);
+                                 ctx->kp, ctx->gord_d, sb, argmin_d, ctx->stream, &ctx->launches);
     else if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_BLEND) && b_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  ctx->kp, ctx->order_d, sb, argmin_d, ctx->stream,
@@ -326,10 +348,36 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
     return PG_OK;
 }
 
+// Waits for the context stream up to the context's time limit (none when
+// it is 0): polls the event recorded after the last queued work.  On
+// PG_ETIMEOUT the work is still queued or running; the context stays usable
+// once it finishes (pg_destroy waits for it).
+int wait_stream(pg_ctx* ctx) {
+    if (!(ctx->wait_timeout_s > 0.0)) {
+        PG_CUDA(cudaStreamSynchronize(ctx->stream));
+        return PG_OK;
+    }
+    PG_CUDA(cudaEventRecord(ctx->ev_wait, ctx->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(ctx->ev_wait);
+        if (e == cudaSuccess) return PG_OK;
+        if (e != cudaErrorNotReady)
+            return fail(PG_ECUDA, std::string("sweep wait: ") + cudaGetErrorString(e));
+        const double el =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > ctx->wait_timeout_s)
+            return fail(PG_ETIMEOUT, "a sweep did not finish within the context's wait limit of " +
+                                         std::to_string(ctx->wait_timeout_s) + " s");
+        std::this_thread::sleep_for(std::chrono::microseconds(el < 1e-3 ? 20 : 200));
+    }
+}
+
 int read_residual(pg_ctx* ctx, double* d, double* dm) {
     PG_CUDA(cudaMemcpyAsync(ctx->red_h, ctx->red_d, 2 * sizeof(double), cudaMemcpyDeviceToHost,
                             ctx->stream));
-    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    int rc = wait_stream(ctx);
+    if (rc) return rc;
     *d = ctx->red_h[0];
     *dm = ctx->red_h[1];
     return PG_OK;
@@ -426,6 +474,7 @@ int pg_create(pg_ctx** out, int device) {
     c->device = device;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_wait, cudaEventDisableTiming) != cudaSuccess ||
         cudaMalloc(&c->red_d, 2 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&c->red_h, 2 * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&c->counts_d, 2 * sizeof(unsigned long long)) != cudaSuccess) {
@@ -446,6 +495,7 @@ int pg_destroy(pg_ctx* ctx) {
     if (ctx->counts_d) cudaFree(ctx->counts_d);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->ev_wait) cudaEventDestroy(ctx->ev_wait);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PG_OK;
@@ -604,47 +654,70 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     if (rb > ctx->nparts) ctx->nparts = rb;
     PG_CUDA(cudaMalloc(&ctx->part_sum, sizeof(double) * ctx->nparts));
     PG_CUDA(cudaMalloc(&ctx->part_max, sizeof(double) * ctx->nparts));
-    // The admissibility mask of the masked stencil: decided once here, read by
-    // every sweep.  Skipped (the row stencil decides per sweep instead) when
-    // it would not leave 4 GiB of device memory free.
+    // The admissibility decisions of the masked stencils, made once here and
+    // read by every sweep: the per-(plane, control) records, the row-order
+    // mask (the re-reading blend, the 64-corner gather, the adjoint) and the
+    // tile-order mask with the corner-group order (the register-resident
+    // blend).  Everything is kept when it leaves 4 GiB free.  Otherwise the
+    // register-resident blend alone is kept when its records and tile mask
+    // fit (the row-order mask is then made a chunk of planes at a time and
+    // dropped), else the row-order mask alone; with neither, the row stencil
+    // decides per sweep.
     if (ctx->stencil_ok && storage != PG_STORE_F64) {
         const size_t mb = pg::stencil_mask_bytes(kp), rb = pg::stencil_recs_bytes(kp);
+        const size_t gb = (size_t)kp.nplanes * kp.nctl * sizeof(uint16_t);
+        const bool r_able = kp.rtile_x > 0 && kp.nctl <= 0x7fff && r_smem_fits(kp);
+        const size_t tb = r_able ? pg::stencil_tmask_bytes(kp) : 0;
+        const size_t G = (size_t)1 << 30;
         size_t fr = 0, tot = 0;
         PG_CUDA(cudaMemGetInfo(&fr, &tot));
-        if (mb + rb + ((size_t)4 << 30) < fr && cudaMalloc(&ctx->mask_d, mb) == cudaSuccess &&
-            cudaMalloc(&ctx->recs_d, rb) == cudaSuccess) {
-            cudaError_t e = pg::launch_stencil_prep(ctx->occ_d, kp, ctx->ctl_d, ctx->mask_d,
-                                                    ctx->recs_d, ctx->stream, &ctx->launches);
+        bool keep_rows = mb + rb + (r_able ? gb + tb : 0) + 4 * G < fr;
+        bool r_only = !keep_rows && r_able && rb + gb + tb + 6 * G < fr;
+        if (!keep_rows && !r_only) keep_rows = mb + rb + 4 * G < fr;
+        cudaError_t e = cudaSuccess;
+        if (keep_rows || r_only) {
+            if (cudaMalloc(&ctx->recs_d, rb) != cudaSuccess ||
+                (keep_rows && cudaMalloc(&ctx->mask_d, mb) != cudaSuccess)) {
+                cudaGetLastError();
+                if (ctx->recs_d) cudaFree(ctx->recs_d);
+                ctx->recs_d = nullptr;
+                ctx->mask_d = nullptr;
+                keep_rows = r_only = false;
+            }
+        }
+        if (keep_rows) {
+            e = pg::launch_stencil_prep(ctx->occ_d, kp, ctx->ctl_d, ctx->mask_d, ctx->recs_d, 0,
+                                        kp.nplanes, ctx->stream, &ctx->launches);
             if (e != cudaSuccess) return fail(PG_ECUDA, std::string("prep: ") + cudaGetErrorString(e));
             ctx->mask_ok = true;
             ctx->blend_ok = kp.btile_x > 0 && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
             ctx->gather_ok = pg::stencil_u_smem_bytes(kp) <= 200 * 1024;
-            // the register-resident blend's per-plane control order,
-            // successor entries and tile-order mask
+        }
+        if ((keep_rows || r_only) && r_able) {
             size_t fr2 = 0, tot2 = 0;
             PG_CUDA(cudaMemGetInfo(&fr2, &tot2));
-            const size_t gb = (size_t)kp.nplanes * kp.nctl * sizeof(uint16_t);
-            const size_t rcb = pg::stencil_rc_bytes(kp);
-            if (kp.rtile_x > 0 && kp.nctl <= 0x7fff && r_smem_fits(kp) &&
-                gb + rcb + pg::stencil_tmask_bytes(kp) + ((size_t)2 << 30) < fr2 &&
-                cudaMalloc(&ctx->gord_d, gb) == cudaSuccess &&
-                cudaMalloc(&ctx->rctab_d, rcb) == cudaSuccess) {
+            if (gb + tb + 2 * G < fr2 && cudaMalloc(&ctx->gord_d, gb) == cudaSuccess) {
+                // the records first (made by the chunked prep when no
+                // row-order mask is kept), then the group order
+                if (!keep_rows) {
+                    int rc2 = build_r_tables(ctx);
+                    if (rc2) return rc2;
+                }
                 e = pg::launch_stencil_group(ctx->recs_d, kp, ctx->order_d, ctx->gord_d,
                                              ctx->stream, &ctx->launches);
                 if (e != cudaSuccess)
                     return fail(PG_ECUDA, std::string("group: ") + cudaGetErrorString(e));
-                int rc2 = build_r_tables(ctx);
-                if (rc2) return rc2;
+                if (keep_rows) {
+                    int rc2 = build_r_tables(ctx);
+                    if (rc2) return rc2;
+                }
             } else {
                 cudaGetLastError();
-                if (ctx->gord_d) cudaFree(ctx->gord_d);
                 ctx->gord_d = nullptr;
-                ctx->rctab_d = nullptr;
             }
-        } else {
-            cudaGetLastError();
-            if (ctx->mask_d) cudaFree(ctx->mask_d);
-            ctx->mask_d = nullptr;
+        }
+        if (!ctx->mask_ok && !ctx->rblend_ok && ctx->recs_d) {
+            cudaFree(ctx->recs_d);
             ctx->recs_d = nullptr;
         }
     }
@@ -951,8 +1024,7 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device, int32_t
     void* spare = ctx->V[1 - ctx->cur];
     if (ctx->rblend_ok)
         e = pg::launch_stencil_r(ctx->storage, vin, spare, ctx->occ_d, ctx->recs_d, ctx->tmask_d,
-                                 ctx->rctab_d, r_cols(ctx), kp, ctx->gord_d, sb, ctx->argmin_d,
-                                 ctx->stream, &ctx->launches);
+                                 kp, ctx->gord_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
     else if (ctx->blend_ok)
         e = pg::launch_stencil_b(ctx->storage, vin, spare, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  kp, ctx->order_d, sb, ctx->argmin_d, ctx->stream, &ctx->launches);
@@ -1170,8 +1242,6 @@ int batch_descriptors(pg_batch* b, int st, std::vector<pg::BatchTable>& d, std::
         t.recs = c->recs_d;
         t.order = c->order_d;
         t.tmask = c->tmask_d;
-        t.rrow = c->rctab_d;
-        t.rcol = c->rctab_d ? r_cols(c) : nullptr;
         t.gord = c->gord_d;
         t.kp = c->kp;
         t.kp.tile_x = use_r ? c->kp.rtile_x : c->kp.btile_x;
@@ -1354,7 +1424,7 @@ int pg_batch_add(pg_batch* b, const pg_grid6* g, const pg_model* m, const pg_par
     if (rc) return rc;
     rc = pg_load_problem(c, g, m, p, occ, ctl, nctl, b->storage);
     if (!rc && tile_rows > 0) rc = pg_set_tile_rows(c, tile_rows);
-    if (!rc && !(c->stencil_ok && c->mask_ok && (c->blend_ok || c->rblend_ok)))
+    if (!rc && !(c->stencil_ok && ((c->mask_ok && c->blend_ok) || c->rblend_ok)))
         rc = fail(PG_EUNSUPPORTED, "a batched table must run a blend-then-shift sweep (" +
                                        (c->stencil_ok ? std::string("its records do not fit")
                                                       : c->stencil_why) + ")");
@@ -1467,6 +1537,14 @@ int pg_batch_table(pg_batch* b, int32_t table, int32_t* sweeps, double* last_max
     if (sweeps) *sweeps = b->sweeps[table];
     if (last_maxnorm) *last_maxnorm = b->last_max[table];
     if (ctx) *ctx = b->tabs[table];
+    return PG_OK;
+}
+
+int pg_set_wait_timeout(pg_ctx* ctx, double seconds) {
+    if (!ctx) return fail(PG_EINVAL, "null context");
+    if (!(seconds >= 0.0) || !std::isfinite(seconds))
+        return fail(PG_EINVAL, "the wait limit must be a finite number of seconds >= 0");
+    ctx->wait_timeout_s = seconds;
     return PG_OK;
 }
 

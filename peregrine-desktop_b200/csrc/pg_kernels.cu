@@ -832,8 +832,8 @@ cudaError_t launch_stencil(int storage, bool exact, const void* Vin, void* Vout,
 }
 
 cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const float* ctl,
-                                uint32_t* mask, uint32_t* recs, cudaStream_t st,
-                                int64_t* launches) {
+                                uint32_t* mask, uint32_t* recs, int64_t plane0, int64_t nplanes,
+                                cudaStream_t st, int64_t* launches) {
     size_t smem = stencil_prep_smem(kp.nctl, kp.nsub);
     const size_t tab = stencil_prep_tab_smem(kp.nctl, kp.g.n[1]);
     const int coltab = kp.g.n[1] <= 255 && kp.nchk <= 4 && smem + tab <= 200 * 1024;
@@ -847,8 +847,10 @@ cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const flo
         if (e != cudaSuccess) return e;
         attr_set.fetch_or(attr_bit);
     }
-    if (kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
-    k_stencil_prep<<<(unsigned)kp.nplanes, 256, smem, st>>>(occ, kp, ctl, mask, recs, coltab);
+    if (plane0 < 0 || nplanes < 0 || plane0 + nplanes > kp.nplanes || nplanes > 0x7fffffffLL)
+        return cudaErrorInvalidValue;
+    if (nplanes == 0) return cudaSuccess;
+    k_stencil_prep<<<(unsigned)nplanes, 256, smem, st>>>(occ, kp, ctl, mask, recs, coltab, plane0);
     *launches += 1;
     return cudaGetLastError();
 }
@@ -1122,20 +1124,19 @@ cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const 
 
 template <typename S, bool ARGMIN, int KR>
 static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
-                               const uint32_t* recs, const uint32_t* tmask, const int2* rrow,
-                               const int2* rcol, const KParams& kp, const uint16_t* gord,
-                               const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
-                               int64_t* launches) {
+                               const uint32_t* recs, const uint32_t* tmask, const KParams& kp,
+                               const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
+                               cudaStream_t st, int64_t* launches) {
     if (kp.rtile_x <= 0 || kp.rblock <= 0 || kp.rblock > RShape<KR>::kMaxThreads ||
-        kp.rblock % 32 != 0 || kp.nsub > kStencilMaxSub || kp.g.n[1] > 0xffff ||
-        (int64_t)(kp.rtile_x + 3) * kp.g.n[1] > (int64_t)kp.rblock * KR)
+        kp.rblock % 32 != 0 || (KR * (kp.rblock / 32)) % 4 != 0 || kp.nsub > kStencilMaxSub ||
+        kp.g.n[1] > 0xffff || (int64_t)(kp.rtile_x + 3) * kp.g.n[1] > (int64_t)kp.rblock * KR)
         return cudaErrorInvalidValue;
     KParams kr = kp;
     kr.tile_x = kp.rtile_x;
     kr.tiles_x = kp.rtiles_x;
     const int64_t blocks = kp.nplanes * kp.rtiles_x;
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-    const size_t smem = stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, KR);
+    const size_t smem = stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, KR, kp.nsub);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
@@ -1146,8 +1147,7 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
         attr_set.fetch_or(attr_bit);
     }
     k_stencil_r<S, ARGMIN, KR><<<(unsigned)blocks, kp.rblock, smem, st>>>(
-        (const S*)Vin, (S*)Vout, occ, recs, tmask, rrow, rcol, kr, gord, sb.part_sum, sb.part_max,
-        argmin);
+        (const S*)Vin, (S*)Vout, occ, recs, tmask, kr, gord, sb.part_sum, sb.part_max, argmin);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
@@ -1156,17 +1156,14 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
 }
 
 cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uint8_t* occ,
-                             const uint32_t* recs, const uint32_t* tmask, const int2* rrow,
-                             const int2* rcol, const KParams& kp, const uint16_t* gord,
-                             const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
-                             int64_t* launches) {
+                             const uint32_t* recs, const uint32_t* tmask, const KParams& kp,
+                             const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
+                             cudaStream_t st, int64_t* launches) {
 #define PG_SR(S)                                                                                 \
-    return argmin ? stencil_r_t<S, true, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rrow,    \
-                                                           rcol, kp, gord, sb, argmin, st,       \
-                                                           launches)                             \
-                  : stencil_r_t<S, false, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, rrow,   \
-                                                            rcol, kp, gord, sb, argmin, st,      \
-                                                            launches)
+    return argmin ? stencil_r_t<S, true, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, kp,      \
+                                                           gord, sb, argmin, st, launches)       \
+                  : stencil_r_t<S, false, kRCellsPerThread>(Vin, Vout, occ, recs, tmask, kp,     \
+                                                            gord, sb, argmin, st, launches)
     switch (storage) {
         case PG_STORE_F32: PG_SR(float);
         case PG_STORE_F16: PG_SR(__half);
@@ -1177,42 +1174,27 @@ cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uin
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_stencil_rc(const uint32_t* recs, const KParams& kp, int2* rrow, int2* rcol,
-                              cudaStream_t st, int64_t* launches) {
-    if (kp.rtile_x <= 0) return cudaErrorInvalidValue;
-    const int64_t total = kp.nplanes * kp.nctl * (kp.g.n[0] + kp.g.n[1]);
-    k_stencil_rc<<<grid_for(total, 256), 256, 0, st>>>(recs, kp, kp.rtile_x, rrow, rcol);
+cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, int64_t plane0,
+                                 int64_t nplanes, uint32_t* tmask, cudaStream_t st,
+                                 int64_t* launches) {
+    if (kp.rtile_x <= 0 || plane0 < 0 || nplanes < 0 || plane0 + nplanes > kp.nplanes)
+        return cudaErrorInvalidValue;
+    if (nplanes == 0) return cudaSuccess;
+    const int32_t ts = tile_mask_stride(kp.rtile_x, kp.g.n[1]);
+    const int64_t total = nplanes * kp.rtiles_x * kp.nctl * ts;
+    k_stencil_tmask<<<grid_for(total, 256), 256, 0, st>>>(mask, kp, kp.rtile_x, kp.rtiles_x, ts,
+                                                          plane0, nplanes, tmask);
     *launches += 1;
     return cudaGetLastError();
-}
-
-cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, uint32_t* tmask,
-                                 cudaStream_t st, int64_t* launches) {
-    if (kp.rtile_x <= 0) return cudaErrorInvalidValue;
-    const int64_t total = stencil_tmask_bytes(kp) / 4;
-    k_stencil_tmask<<<grid_for(total, 256), 256, 0, st>>>(mask, kp, kp.rtile_x, kp.rtiles_x,
-                                                          stencil_r_mask_words(kp), tmask);
-    *launches += 1;
-    return cudaGetLastError();
-}
-
-size_t stencil_rc_bytes(const KParams& kp) {
-    return (size_t)kp.nplanes * kp.nctl * (kp.g.n[0] + kp.g.n[1]) * sizeof(int2);
-}
-
-// mask words per control of the register-resident sweep: one per warp and
-// cell slot
-int32_t stencil_r_mask_words(const KParams& kp) {
-    return kRCellsPerThread * (kp.rblock / 32);
 }
 
 size_t stencil_tmask_bytes(const KParams& kp) {
-    return (size_t)kp.nplanes * kp.rtiles_x * kp.nctl * stencil_r_mask_words(kp) *
+    return (size_t)kp.nplanes * kp.rtiles_x * kp.nctl * tile_mask_stride(kp.rtile_x, kp.g.n[1]) *
            sizeof(uint32_t);
 }
 
 size_t stencil_r_smem_bytes(const KParams& kp) {
-    return stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, kRCellsPerThread);
+    return stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, kRCellsPerThread, kp.nsub);
 }
 
 size_t stencil_b_smem_bytes(const KParams& kp) {

@@ -33,9 +33,11 @@ cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t
                           double scale, double escape_scale, int64_t lo, int64_t n, uint8_t* out,
                           unsigned long long* counts, cudaStream_t st);
 
+// Records of the planes [plane0, plane0 + nplanes) into recs (indexed by
+// plane), their row-order mask words into `mask` (plane plane0 first).
 cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const float* ctl,
-                                uint32_t* mask, uint32_t* recs, cudaStream_t st,
-                                int64_t* launches);
+                                uint32_t* mask, uint32_t* recs, int64_t plane0, int64_t nplanes,
+                                cudaStream_t st, int64_t* launches);
 cudaError_t launch_stencil_u(int storage, const void* Vin, void* Vout, const uint8_t* occ,
                              const uint32_t* mask, const uint32_t* recs, const KParams& kp,
                              const int32_t* order, const SweepBufs& sb, int16_t* argmin,
@@ -48,17 +50,15 @@ size_t stencil_b_smem_bytes(const KParams& kp);
 cudaError_t launch_stencil_group(const uint32_t* recs, const KParams& kp, const int32_t* order,
                                  uint16_t* gord, cudaStream_t st, int64_t* launches);
 cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uint8_t* occ,
-                             const uint32_t* recs, const uint32_t* tmask, const int2* rrow,
-                             const int2* rcol, const KParams& kp, const uint16_t* gord,
-                             const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
-                             int64_t* launches);
-cudaError_t launch_stencil_rc(const uint32_t* recs, const KParams& kp, int2* rrow, int2* rcol,
-                              cudaStream_t st, int64_t* launches);
-int32_t stencil_r_mask_words(const KParams& kp);
-cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, uint32_t* tmask,
-                                 cudaStream_t st, int64_t* launches);
+                             const uint32_t* recs, const uint32_t* tmask, const KParams& kp,
+                             const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
+                             cudaStream_t st, int64_t* launches);
+// Tile-order mask of the planes [plane0, plane0 + nplanes) from their row-order
+// words in `mask` (plane plane0 first).
+cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, int64_t plane0,
+                                 int64_t nplanes, uint32_t* tmask, cudaStream_t st,
+                                 int64_t* launches);
 size_t stencil_r_smem_bytes(const KParams& kp);
-size_t stencil_rc_bytes(const KParams& kp);
 size_t stencil_tmask_bytes(const KParams& kp);
 cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
                                    int64_t count, int threads, int parity, const int32_t* done,

@@ -14,19 +14,20 @@
 //   (corner planes, x offset) and flags the first control of each group;
 //   controls that no cell of the plane admits go last;
 //
-//   k_stencil_rc (once per tiling) stores each (plane, control, row)'s and
-//   each (plane, control, column)'s successor corner and fraction -- which
-//   k_stencil_b recomputes every sweep -- in the form the sweep reads them,
-//   and k_stencil_tmask (once per tiling) regroups the admissibility mask per
+//   k_stencil_tmask (once per tiling) regroups the admissibility mask per
 //   (plane, tile, control) in tile order;
 //
 //   k_stencil_r copies a block's per-control data (weights, tau, offsets,
-//   mask words, successor entries) into shared memory with asynchronous
-//   copies, loads at the first control of each group the 16 corner values
-//   of each of its window cells into registers (KR cells per thread), and
-//   for every control of the group blends them with the control's 16
-//   weights -- 16 FMAs per window cell from registers, nothing re-read --
-//   into the shared window, then shifts exactly as k_stencil_b does.
+//   substep increments, mask words) into shared memory with asynchronous
+//   copies, computes from the staged increments every control's per-row and
+//   per-column successor corners and fractions (which k_stencil_b
+//   recomputes per control; here many independent chains per thread, once
+//   per block), loads at the first control of each group the 16 corner
+//   values of each of its window cells into registers (KR cells per
+//   thread), and for every control of the group blends them with the
+//   control's 16 weights -- 16 FMAs per window cell from registers, nothing
+//   re-read -- into the shared window, then shifts exactly as k_stencil_b
+//   does.
 //
 // The arithmetic is k_stencil_b's, operation for operation: the same FMA
 // chain over the corners in record order, the same per-row / per-column
@@ -117,15 +118,15 @@ __global__ void __launch_bounds__(128)
 // inc_1 + ... + inc_nsub one add at a time, then (x' - lo) / step and its
 // floor (PeregrineSolver.jl:248-279, 399-431).  li is clamped to
 // [-2, n + 2]: successors off the table are never admissible, and the clamp
-// only keeps their (unused) indices small.
-__device__ __forceinline__ void succ_li_t(const GridT<float>& g, const float* inc, int nsub,
-                                          bool row, int32_t idx, int32_t n1, int32_t n2,
-                                          int32_t* li, float* t) {
+// only keeps their (unused) indices small.  Reads the grid from the kernel
+// parameters, so it costs no registers for the grid.
+__device__ __forceinline__ void succ_li_t(const pg_grid6& g, const float* inc, int nsub, bool row,
+                                          int32_t idx, int32_t n1, int32_t n2, int32_t* li,
+                                          float* t) {
     typedef Ar<float> R_;
-    const float x = row ? axisvalue(g, 0, idx) : axisvalue(g, 1, idx);
     const float lo = row ? g.lo[0] : g.lo[1];
     const float st = row ? g.step[0] : g.step[1];
-    float xn = x;
+    float xn = R_::add(lo, R_::mul((float)idx, st));  // axisvalue
     for (int k = 0; k < nsub; ++k) xn = R_::add(xn, inc[k]);
     const float f = R_::div(R_::sub(xn, lo), st);
     const float fl = floorf(f);
@@ -133,64 +134,28 @@ __device__ __forceinline__ void succ_li_t(const GridT<float>& g, const float* in
     *li = (int32_t)fminf(fmaxf(fl, -2.0f), (float)(row ? n1 + 2 : n2 + 2));
 }
 
-// Once per tiling: the successor entries of every (plane, control) in the
-// form the sweep reads them.  Rows (rrow, n1 per pair): (window offset, x
-// fraction), the window offset = (li - wbase) clamped to the window of the
-// row's tile, times the window row stride n2 + 1, with wbase = x0 + ox - 1
-// for the tile's first row x0 and the control's nominal x offset ox.
-// Columns (rcol, n2 per pair): (li clamped to the columns, y fraction).
-// Inadmissible controls get (0, 0), never read.
-__global__ void k_stencil_rc(const uint32_t* __restrict__ recs, KParams kp, int32_t tile_x,
-                             int2* __restrict__ rrow, int2* __restrict__ rcol) {
-    const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], per = n1 + n2, SB = n2 + 1;
-    GridT<float> g;
-    load_grid(g, kp.g);
-    const int64_t total = kp.nplanes * kp.nctl * per;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t pu = i / per;
-        const int32_t it = (int32_t)(i - pu * per);
-        const bool row = it < n1;
-        const int32_t idx = row ? it : it - n1;
-        int2* dst = row ? rrow + pu * n1 + idx : rcol + pu * n2 + idx;
-        const uint32_t* rec = recs + (size_t)pu * kURec;
-        if (__ldg(rec + kUNT + 18) == 0u) {
-            *dst = make_int2(0, 0);
-            continue;
-        }
-        const float* inc = reinterpret_cast<const float*>(rec + kUInc) + (row ? 0 : kStencilMaxSub);
-        int32_t li;
-        float t;
-        succ_li_t(g, inc, (int)__ldg(rec + kUNT + 19), row, idx, n1, n2, &li, &t);
-        if (row) {
-            const int32_t x0 = (idx / tile_x) * tile_x;
-            const int32_t nw = min(tile_x, n1 - x0) + 3;
-            const int32_t wbase = x0 + (int32_t)__ldg(rec + kUNT + 16) - 1;
-            *dst = make_int2(min(max(li - wbase, 0), nw - 2) * SB, __float_as_int(t));
-        } else {
-            *dst = make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
-        }
-    }
-}
-
 // Words of one tile's admissibility bits in tile order (bit e of the tile =
-// cell e = a * n2 + j of its rows), per control.
-__host__ __device__ inline int32_t tile_mask_words(int32_t tile_x, int32_t n2) {
-    return (tile_x * n2 + 31) / 32;
+// cell e = a * n2 + j of its rows), rounded up to whole 16-byte pieces: the
+// stride of one (plane, tile, control)'s words in the tile-order mask.
+__host__ __device__ inline int32_t tile_mask_stride(int32_t tile_x, int32_t n2) {
+    return ((tile_x * n2 + 31) / 32 + 3) & ~3;
 }
 
-// Once per tiling: the admissibility mask regrouped per (plane, tile,
-// control) in tile order, from the per-row layout of k_stencil_prep; mws
-// words per control (the sweep's words per control, zero past the tile).
+// The admissibility mask regrouped per (plane, tile, control) in tile order,
+// from the per-row layout of k_stencil_prep, for the planes [plane0,
+// plane0 + nplanes) whose row-order words `mask` holds (plane plane0 first);
+// tstride words per control, zero past the tile's cells.
 __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, int32_t tile_x,
-                                int32_t tiles_x, int32_t mws, uint32_t* __restrict__ tmask) {
+                                int32_t tiles_x, int32_t tstride, int64_t plane0, int64_t nplanes,
+                                uint32_t* __restrict__ tmask) {
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1], W = mask_words(n2);
     const int nctl = kp.nctl;
-    const int64_t total = kp.nplanes * tiles_x * nctl * mws;
+    const int64_t total = nplanes * tiles_x * nctl * tstride;
+    uint32_t* out = tmask + (size_t)plane0 * tiles_x * nctl * tstride;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t r = i / mws;
-        const int32_t w = (int32_t)(i - r * mws);
+        int64_t r = i / tstride;
+        const int32_t w = (int32_t)(i - r * tstride);
         const int32_t u = (int32_t)(r % nctl);
         r /= nctl;
         const int32_t xt = (int32_t)(r % tiles_x);
@@ -217,26 +182,29 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
             j = 0;
             ++a;
         }
-        tmask[i] = word;
+        out[i] = word;
     }
 }
 
 // Shared memory of one k_stencil_r block of `threads` threads (a multiple of
 // 32) with KR cells per thread: the plane's group order; per control its
-// record's weights, tau, offsets, admissibility and substeps (24 words), its
-// mask words (one per warp and cell slot: the tile's words, zero beyond them)
-// and its successor entries; and two padded window buffers with room for
-// every thread's KR window slots (slots past the window land in scratch rows).
+// record's weights, tau, offsets, admissibility and substeps (24 words) and
+// its substep position increments (x, then y, each rounded up to 4 words);
+// its mask words (one per warp and cell slot: the tile's words, zero beyond
+// them) and its successor entries (the tile's rows, then every column); and
+// two padded window buffers with room for every thread's KR window slots
+// (slots past the window land in scratch rows).
 constexpr int kRWt = 24;  // w[16], tau, tx, ty, -, ox, oy, ok, nsub
+__host__ __device__ inline int32_t stencil_r_ninc(int nsub) { return (nsub + 3) & ~3; }
 __host__ __device__ inline int32_t stencil_r_window_rows(int tile_x, int n2, int threads, int kr) {
     const int32_t slots = (kr * threads + n2 - 1) / n2;
     return slots > tile_x + 3 ? slots : tile_x + 3;
 }
-__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2, int threads,
-                                                 int kr) {
+__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2, int threads, int kr,
+                                                 int nsub) {
     return (size_t)((nctl + 7) & ~7) * 2 + (size_t)nctl * kRWt * 4 +
-           (size_t)nctl * kr * (threads / 32) * 4 + 4 +
-           (size_t)nctl * (tile_x + n2) * 2 * sizeof(int32_t) +
+           (size_t)nctl * 2 * stencil_r_ninc(nsub) * 4 + (size_t)nctl * kr * (threads / 32) * 4 +
+           (size_t)nctl * (tile_x + n2) * sizeof(int2) +
            2 * (size_t)stencil_r_window_rows(tile_x, n2, threads, kr) * (n2 + 1) * sizeof(float);
 }
 
@@ -248,8 +216,7 @@ __host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2, i
 template <typename S, bool ARGMIN, int KR>
 __device__ __forceinline__ void stencil_r_item(
     const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
-    const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
-    const int2* __restrict__ rrow, const int2* __restrict__ rcol, const KParams& kp,
+    const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask, const KParams& kp,
     const uint16_t* __restrict__ gord, double* part_sum, double* part_max, int16_t* argmin,
     int64_t item, int64_t slot, unsigned char* smem_raw) {
     const int nctl = kp.nctl;
@@ -261,14 +228,17 @@ __device__ __forceinline__ void stencil_r_item(
     const int32_t bsz = stencil_r_window_rows(TX, n2, T, KR) * SB;
     const int32_t mwq = T >> 5;          // mask words per cell slot
     const int32_t MWS = KR * mwq;        // mask words per control in shared memory
-    const int32_t rcs = TX + n2;  // successor entries per control
+    const int32_t TS = tile_mask_stride(TX, n2);  // mask words per control in the tile mask
+    const int32_t NI = stencil_r_ninc(kp.nsub);   // increments per axis in shared memory
+    const int32_t ecs = TX + n2;  // successor entries per control
     uint16_t* ord = reinterpret_cast<uint16_t*>(smem_raw);
     float* wt = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));  // [nctl][kRWt]
-    uint32_t* msk = reinterpret_cast<uint32_t*>(wt + nctl * kRWt);   // [nctl][MWS]
-    // [nctl][rcs]: TX rows (window offset, x fraction), n2 columns (column,
+    float* incs = wt + nctl * kRWt;                                   // [nctl][2 NI]
+    uint32_t* msk = reinterpret_cast<uint32_t*>(incs + nctl * 2 * NI);  // [nctl][MWS]
+    // [nctl][ecs]: TX rows (window offset, x fraction), n2 columns (column,
     // y fraction)
-    int2* rcinfo = reinterpret_cast<int2*>(msk + nctl * MWS + ((nctl * MWS) & 1));
-    float* Bbuf = reinterpret_cast<float*>(rcinfo + nctl * rcs);
+    int2* ent = reinterpret_cast<int2*>(msk + nctl * MWS);
+    float* Bbuf = reinterpret_cast<float*>(ent + (size_t)nctl * ecs);
     const Layout L = make_layout(kp);
     const float cap = kp.p.cap;
     const int64_t P = L.P;
@@ -290,24 +260,32 @@ __device__ __forceinline__ void stencil_r_item(
     // stage the block's per-control data with asynchronous copies, waited
     // for once below: per control its record's words 0-19 (w[16], tau, tx,
     // ty, -) and kUNT+16..19 (ox, oy, ok, nsub) as six 16-byte pieces, its
-    // mask words, its row and column successor entries
+    // first NI x and y increments, and its mask words (zero past the tile's)
     for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
     for (int i = tid; i < nctl * 6; i += T) {
         const int u = i / 6, c = i - u * 6;
         cp_async16(wt + u * kRWt + 4 * c, prec + (size_t)u * kURec + (c < 5 ? 4 * c : kUNT + 16));
     }
     {
-        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * MWS;
-        for (int i = tid; i < nctl * MWS / 4; i += T) cp_async16(msk + 4 * i, src + 4 * i);
+        const int32_t pieces = NI / 2;  // 16-byte pieces per control: NI/4 for x, NI/4 for y
+        for (int i = tid; i < nctl * pieces; i += T) {
+            const int u = i / pieces, c = i - u * pieces;
+            const int32_t half = NI / 4;
+            const int32_t src = c < half ? kUInc + 4 * c : kUInc + kStencilMaxSub + 4 * (c - half);
+            cp_async16(incs + u * 2 * NI + 4 * c, prec + (size_t)u * kURec + src);
+        }
     }
     {
-        const int32_t per = nr + n2;
-        for (int32_t i = tid; i < nctl * per; i += T) {
-            const int32_t u = i / per, it = i - u * per;
-            const bool row = it < nr;
-            const int2* src = row ? rrow + ((size_t)pl * nctl + u) * n1 + x0 + it
-                                  : rcol + ((size_t)pl * nctl + u) * n2 + (it - nr);
-            cp_async8(rcinfo + (size_t)u * rcs + (row ? it : TX + it - nr), src);
+        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * TS;
+        const int32_t p4 = TS / 4;
+        for (int i = tid; i < nctl * p4; i += T) {
+            const int u = i / p4, c = i - u * p4;
+            cp_async16(msk + u * MWS + 4 * c, src + (size_t)u * TS + 4 * c);
+        }
+        const int32_t zw = MWS - TS;
+        for (int i = tid; i < nctl * zw; i += T) {
+            const int u = i / zw;
+            msk[u * MWS + TS + (i - u * zw)] = 0u;
         }
     }
     cp_async_commit();
@@ -347,6 +325,28 @@ __device__ __forceinline__ void stencil_r_item(
     cp_async_wait_all();
     __syncthreads();
 
+    // every admissible control's successor entries from its staged
+    // increments: rows (the window offset of the lower corner, the x
+    // fraction), then columns (the lower column, the y fraction).  Many
+    // independent chains per thread, all from shared memory.
+    for (int32_t i = tid; i < nctl * ecs; i += T) {
+        const int u = i / ecs;
+        const int32_t k = i - u * ecs;
+        if (__float_as_uint(wt[u * kRWt + 22]) == 0u || (k >= nr && k < TX)) continue;
+        const bool row = k < TX;
+        int32_t li;
+        float t;
+        succ_li_t(kp.g, incs + u * 2 * NI + (row ? 0 : NI), kp.nsub, row,
+                  row ? x0 + k : k - TX, n1, n2, &li, &t);
+        if (row) {
+            const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 20]) - 1;
+            ent[i] = make_int2(min(max(li - wbase, 0), nr + 1) * SB, __float_as_int(t));
+        } else {
+            ent[i] = make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
+        }
+    }
+    __syncthreads();
+
     static_assert(KR % 2 == 0, "window slots are paired for the packed FMA");
     uint64_t cv[KR / 2][16];  // the group's corner values, slots 2i and 2i+1 paired
     // corner values of the group that control uu starts: the planes of its
@@ -375,8 +375,8 @@ __device__ __forceinline__ void stencil_r_item(
     if (__float_as_uint(wt[(ord[0] & 0x7fff) * kRWt + 22]) != 0u) load_group(0);
     int buf = 0;
     for (int uu = 0; uu < nctl; ++uu) {
-        const uint32_t ent = ord[uu];
-        const int u = (int)(ent & 0x7fffu);
+        const uint32_t ent_u = ord[uu];
+        const int u = (int)(ent_u & 0x7fffu);
         const float* wu = wt + u * kRWt;
         if (__float_as_uint(wu[22]) == 0u) {
             // no cell of the plane admits this control (block-uniform)
@@ -429,7 +429,7 @@ __device__ __forceinline__ void stencil_r_item(
         // slot (entries are clamped into the window, dead slots read cell
         // (0, 0)), kept where the cell is free and the control admissible
         const float tau = wu[16];
-        const int2* ri = rcinfo + u * rcs;
+        const int2* ri = ent + (size_t)u * ecs;
         const int2* ci = ri + TX;
         const uint32_t* mu = msk + u * MWS + mw0;
 #pragma unroll
@@ -491,13 +491,12 @@ __device__ __forceinline__ void stencil_r_item(
 template <typename S, bool ARGMIN, int KR>
 __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
     k_stencil_r(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
-                const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask,
-                const int2* __restrict__ rrow, const int2* __restrict__ rcol, KParams kp,
+                const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask, KParams kp,
                 const uint16_t* __restrict__ gord, double* part_sum, double* part_max,
                 int16_t* argmin) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    stencil_r_item<S, ARGMIN, KR>(Vin, Vout, occ, recs, tmask, rrow, rcol, kp, gord, part_sum,
-                                  part_max, argmin, blockIdx.x, blockIdx.x, smem_raw);
+    stencil_r_item<S, ARGMIN, KR>(Vin, Vout, occ, recs, tmask, kp, gord, part_sum, part_max,
+                                  argmin, blockIdx.x, blockIdx.x, smem_raw);
 }
 
 // Many tables in one launch, as k_stencil_b_batch (pg_stencil_b.cuh) but
@@ -535,8 +534,7 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         }
         const S* vin = static_cast<const S*>(tb.V[parity]);
         S* vout = const_cast<S*>(static_cast<const S*>(tb.V[1 - parity]));
-        stencil_r_item<S, false, KR>(vin, vout, tb.occ, tb.recs, tb.tmask, tb.rrow, tb.rcol,
-                                     tb.kp, tb.gord, part_sum, part_max, nullptr, it - tb.item0,
-                                     it, smem_raw);
+        stencil_r_item<S, false, KR>(vin, vout, tb.occ, tb.recs, tb.tmask, tb.kp, tb.gord,
+                                     part_sum, part_max, nullptr, it - tb.item0, it, smem_raw);
     }
 }

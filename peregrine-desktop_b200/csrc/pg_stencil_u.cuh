@@ -60,7 +60,8 @@ constexpr uint32_t kPrepColOff = 0xffffffffu;
 // side and the occupancy lookups.  The decisions are the same either way.
 __global__ void __launch_bounds__(256)
     k_stencil_prep(const uint8_t* __restrict__ occ, KParams kp, const float* __restrict__ ctl,
-                   uint32_t* __restrict__ mask, uint32_t* __restrict__ recs, int coltab) {
+                   uint32_t* __restrict__ mask, uint32_t* __restrict__ recs, int coltab,
+                   int64_t plane0) {
     typedef Ar<float> R_;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nctl = kp.nctl, nsub = kp.nsub, nchk = kp.nchk;
@@ -71,7 +72,10 @@ __global__ void __launch_bounds__(256)
     const Layout L = make_layout(kp);
     GridT<float> g;
     load_grid(g, kp.g);
-    const int64_t pl = blockIdx.x;
+    // block = plane plane0 + blockIdx.x; its mask rows go to `mask` at the
+    // block's place (mask holds the planes from plane0 on)
+    const int64_t pl = plane0 + blockIdx.x;
+    const int64_t ml = blockIdx.x;
     int32_t i3, i4, i5, i6;
     {
         int64_t q = pl;
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(256)
                     }
                 }
             }
-            mask[((pl * nctl + u) * n1 + i1) * W + w] = bits;
+            mask[((ml * nctl + u) * n1 + i1) * W + w] = bits;
         }
         return;
     }
@@ -233,7 +237,7 @@ __global__ void __launch_bounds__(256)
                 }
             }
         }
-        mask[((pl * nctl + u) * n1 + i1) * W + w] = bits;
+        mask[((ml * nctl + u) * n1 + i1) * W + w] = bits;
     }
 }
 

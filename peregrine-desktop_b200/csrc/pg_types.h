@@ -76,8 +76,6 @@ struct BatchTable {
     const uint32_t* recs;
     const int32_t* order;
     const uint32_t* tmask;   // register-resident sweep: tile-order mask
-    const int2* rrow;        // register-resident sweep: row successor entries
-    const int2* rcol;        // register-resident sweep: column successor entries
     const uint16_t* gord;    // register-resident sweep: group order
     int64_t item0, nitems;
     int32_t vec;

@@ -35,7 +35,7 @@ EXPORTS = (
     "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
     "pg_launch_count", "pg_set_tile_rows", "pg_batch_create", "pg_batch_destroy",
     "pg_batch_add", "pg_batch_solve", "pg_batch_table", "pg_adjoint", "pg_measure_peaks",
-    "pg_sweep_noalloc", "pg_probe_step", "pg_probe_traction_gain", "pg_probe_interp",
+    "pg_sweep_noalloc", "pg_set_wait_timeout", "pg_probe_step", "pg_probe_traction_gain", "pg_probe_interp",
 )
 
 
@@ -140,6 +140,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "pg_measure_peaks": (C.c_int, [C.c_int, P(f64), P(f64), P(f64)]),
         "pg_sweep_noalloc": (C.c_int, [P(Grid6), P(Model), P(Params), vp, vp, i32, vp, vp, i32,
                                        vp, P(f64), P(f64)]),
+        "pg_set_wait_timeout": (C.c_int, [vp, f64]),
         "pg_probe_step": (C.c_int, [C.c_int, P(Model), i32, vp, vp, vp, vp, i64, vp]),
         "pg_probe_traction_gain": (C.c_int, [C.c_int, vp, C.c_float, i64, vp]),
         "pg_probe_interp": (C.c_int, [vp, vp, i64, i32, i32, i32, C.c_float, vp, vp]),
@@ -301,6 +302,11 @@ class Context:
         n = C.c_int64()
         _check(self._lib.pg_launch_count(self._h, C.byref(n)))
         return n.value
+
+    def set_wait_timeout(self, seconds: float) -> None:
+        """Limit each wait for a sweep (0 = no limit); a sweep that outlasts it
+        makes the solve raise PeregrineError with code PG_ETIMEOUT."""
+        _check(self._lib.pg_set_wait_timeout(self._h, float(seconds)))
 
     def probe_interp(self, states, kuhn=False, nearest=False, vclamp=False, cap=None,
                      grads=False):

@@ -1,6 +1,6 @@
 """Command line, mirroring solver/solve.jl:23-61.
 
-    solve.py <config.json> [plan|solve]
+    solve.py <config.json> [plan|solve|honing [run_dir]]
     solve.py --self-test
 
 Exit 0 on success, 1 on an error (printed as `ERROR <msg>` on stderr with a
@@ -9,6 +9,7 @@ short traceback), 2 on a usage error.
 from __future__ import annotations
 
 import json
+import os
 import sys
 import traceback
 
@@ -38,7 +39,12 @@ def main(argv=None) -> int:
             from .run import run_solve
             run_solve(cfg)
         elif mode == "honing":
-            raise NotImplementedError("honing: the PID derivation is not part of this solver")
+            from .honing import honing_only
+            run_dir = argv[2] if len(argv) >= 3 else None
+            h = honing_only(cfg, write_dir=run_dir)
+            print("HONING " + json.dumps(h))
+            if run_dir is not None:
+                print("WROTE " + os.path.join(run_dir, "MODEL.JSON"))
         else:
             print(f"unknown mode '{mode}' (expected plan, solve or honing)", file=sys.stderr)
             return 2

@@ -45,8 +45,11 @@ def _utc_now() -> str:
 
 
 def model_json(m, reg_path, zeroed_c: bool, cfg=None) -> dict:
-    """model_json (Run.jl:1278-1378) without the honing block: the table is
-    solved and written in full; the PID derivation is not part of the solve."""
+    """model_json (Run.jl:1278-1378): the dynamics model as the solve used
+    it, in the card's over-general block form, plus the honing PID block
+    (honing.py).  Refuses a model whose blocks would make the dynamics
+    depend on position."""
+    from .honing import honing_gains
     Am = [[float(m.A[r, c]) for c in range(3)] for r in range(3)]
     Bm = [[float(m.B[r, c]) for c in range(3)] for r in range(3)]
     Sm = [[float(m.S[r, c]) for c in range(3)] for r in range(3)]
@@ -61,6 +64,10 @@ def model_json(m, reg_path, zeroed_c: bool, cfg=None) -> dict:
     def nz(blk):
         return any(any(v != 0 for v in row) for row in blk)
 
+    for nm, blk in (("A_s", A_s), ("A_ss", A_ss), ("A_sgn", A_sgn), ("A_absv", A_abs)):
+        if any(v != 0 for row in blk for v in row[:3]):
+            raise ValueError(f"{nm} has a non-zero x/y/h column; the dynamics must not depend "
+                             "on where the robot is")
     blocks = [("A_s", nz(A_s)), ("A_u", nz(Bm)), ("A_ss", nz(A_ss)), ("A_uu", nz(A_uu)),
               ("A_sgn", nz(A_sgn)), ("A_absv", nz(A_abs)), ("k", any(v != 0 for v in k))]
     return {
@@ -103,6 +110,7 @@ def model_json(m, reg_path, zeroed_c: bool, cfg=None) -> dict:
         "k": k,
         "constant_zeroed": bool(zeroed_c),
         "nonzero_blocks": [b for b, f in blocks if f],
+        "honing": honing_gains(m, cfg or {}),
     }
 
 
@@ -355,30 +363,157 @@ def run_solve(cfg, device: int = 0) -> dict:
     mj = model_json(prep.model, prep.reg_path, prep.zero_c, cfg)
     with open(os.path.join(out_dir, "MODEL.JSON"), "w") as fh:
         json.dump(mj, fh, indent=2)
+    hn = mj["honing"]
     progress(phase="model", file="MODEL.JSON", nonzero_blocks=mj["nonzero_blocks"],
-             honing_omega=None, honing_budget_frac=None, honing_bound_by=None)
+             honing_omega=hn["omega"], honing_budget_frac=hn["config"]["budget_frac"],
+             honing_bound_by=hn["omega_limits"]["bound_by"])
     progress(phase="done", out_dir=out_dir, targets=len(entries))
     return manifest
 
 
+# Measured sweep rates on one B200 (cell-control updates per second), the
+# cost model of the `runtime` estimate: the plain scheme runs the stencil
+# sweep; any other scheme the one-thread-per-cell kernel of the reference's
+# cell_update.  Ceiling estimates, like the reference's (Run.jl:846-958).
+RATE_STENCIL = 3.0e11
+RATE_CELLFORM = 4.0e9
+
+
+def _gpu_memory(device: int = 0):
+    """(free, total) bytes of the device, or None without a driver."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            mi = pynvml.nvmlDeviceGetMemoryInfo(h)
+            return int(mi.free), int(mi.total)
+        finally:
+            pynvml.nvmlShutdown()
+    except Exception:
+        return None
+
+
+def _stencil_scheme(r) -> bool:
+    """Whether the position-invariant stencil sweep runs this scheme (the
+    library's own test at load time)."""
+    return (r["cfl"] <= 0 and r["ntau"] <= 1 and r["rounds"] <= 0 and not r["achecks"]
+            and not r["nearest"] and not r["simplex"])
+
+
 def plan(cfg) -> dict:
-    """A reduced plan (Run.jl:699-959): the size and fit figures the wizard
-    reads, computed from the same grid construction as the solve."""
+    """plan (Run.jl:699-959): what a solve of this config would build and
+    cost, without solving -- the keys the wizard reads (sizes, span, the
+    occupancy, per-target seeding, the device fit, the grid balance, a
+    runtime ceiling).  Advice this solver has no basis for (the reference's
+    resolution search and tiled-horizon scan) is reported as absent."""
+    from .grid import grid_resolution
+    from .seeds import free_seed_count, seeds_for
+
     prep = Prepared(cfg)
     g, sp = prep.g, prep.sp
+    gcfg = getc(cfg, "grid", {})
+    eb = DTYPES[prep.dtype]["bytes"]
+    cells = prep.cells
+    ntg = len(prep.names)
     elem = {"fp32": 4, "fp16": 2, "bf16": 2, "q16": 2, "fp64": 8}[sp.storage]
-    need = 2 * prep.cells * elem + (3 * prep.cells if sp.warm else 0)
+    occ = prep.occupancy()
+    nh = g.n[2]
+    per_h = [float(np.count_nonzero(occ[k::nh])) / (occ.size / nh) for k in range(nh)]
+    # the device bytes of a solve: two value buffers, the warm-start policy,
+    # and (plain scheme) the stencil's records and tile-order mask
+    need = 2 * cells * elem + (3 * cells if sp.warm else 0)
+    r = sp.raw
+    stencil = _stencil_scheme(r)
+    if stencil:
+        planes = cells // (g.n[0] * g.n[1])
+        need += planes * sp.nctl * (288 + 2 + (g.n[0] * g.n[1] + 31) // 32 * 4)
+    mem = _gpu_memory()
+    fits = mem is not None and need <= mem[0]
+    targets = []
+    for name, st in zip(prep.names, prep.states):
+        seeds = seeds_for(g, st, sp, cfg)
+        nfree = free_seed_count(g, occ, seeds)
+        off = []
+        for k in (0, 1, 3, 4, 5):
+            hi = float(g.lo[k]) + float(g.step[k]) * (g.n[k] - 1)
+            if float(st[k]) < float(g.lo[k]) - 1e-6 or float(st[k]) > hi + 1e-6:
+                off.append(AXES[k])
+        targets.append({"name": name, "ok": nfree > 0, "seed_cells": int(len(seeds)),
+                        "free_seed_cells": int(nfree), "off_axes": off,
+                        "blocked_by": [] if nfree > 0 or off else ["an obstacle or the wall"]})
+    B = np.asarray(prep.model.B, np.float64)
+    acc = max(float(np.max(np.abs(B[0]))), float(np.max(np.abs(B[1]))))
+    dv = float(min(g.step[3], g.step[4]))
+    cell_cm = float(min(g.step[0], g.step[1]))
+    dvd = dv * dv / (2 * acc) if acc > 0 else float("nan")
+    rate = RATE_STENCIL if stencil else RATE_CELLFORM
+    esc = int(getc(cfg, "escape_iterations", 60)) if bool(getc(cfg, "escape", True)) else 0
+    unit_s = cells * sp.nctl / rate
+    blocked = float(np.count_nonzero(occ)) / max(occ.size, 1)
+    runtime = {"unit": "sweep", "unit_s": unit_s, "units": sp.iters + esc,
+               "escape_sweeps": esc, "escape_unit_s": unit_s * (1.0 - blocked),
+               "blocked_frac": blocked, "total_s": unit_s * (sp.iters + esc) * ntg,
+               "rate_cell_controls_per_s": rate,
+               "rate_source": "measured on one B200: the " +
+                              ("stencil sweep (plain scheme)" if stencil else
+                               "cell-form sweep (the reference's cell_update)")}
+    xyres = grid_resolution(gcfg)
+    span_x = float(g.step[0]) * (g.n[0] - 1)
+    span_y = float(g.step[1]) * (g.n[1] - 1)
+    b = prep.bounds
     return {
-        "cells": prep.cells,
+        "cells": cells,
+        "axes": list(AXES),
         "n": list(g.n),
-        "controls": sp.nctl,
-        "bytes_per_target": prep.cells * DTYPES[prep.dtype]["bytes"],
-        "card_bytes": prep.cells * DTYPES[prep.dtype]["bytes"] * len(prep.names),
-        "device_bytes": need,
-        "out_of_core": False,
-        "driver": "whole_grid",
-        "targets": len(prep.names),
-        "resolution": {"xy_cm": float(min(g.step[0], g.step[1])),
-                       "heading_deg": math.degrees(float(g.step[2])),
+        "bounds": {
+            "field": [float(v) for v in b],
+            "table_min": [float(g.lo[k]) for k in range(6)],
+            "table_max": [float(g.lo[k]) + float(g.step[k]) * (g.n[k] if k == 2 else g.n[k] - 1)
+                          for k in range(6)],
+            "inset_cm": [float(g.lo[0]) - b[0], float(g.lo[1]) - b[1],
+                         b[2] - (float(g.lo[0]) + span_x), b[3] - (float(g.lo[1]) + span_y)],
+            "cells_saved_frac": 1.0 - span_x * span_y / max((b[2] - b[0]) * (b[3] - b[1]), 1e-9),
+            "wall_clearance_cm": prep.gi["wall_clearance"],
+            "clearance_cm": prep.gi["clearance"],
+        },
+        "resolution": {
+            "requested": {"xy_cm": xyres[0], "heading_deg": xyres[1], "v_cm_s": xyres[2],
+                          "w_rad_s": xyres[3]},
+            "actual": {"xy_cm": cell_cm, "heading_deg": math.degrees(float(g.step[2])),
                        "v_cm_s": float(g.step[3]), "w_rad_s": float(g.step[5])},
+            "pinned_by_n": getc(gcfg, "n", None) is not None,
+        },
+        "occupancy": {"blocked_frac": blocked, "blocked_cells": int(np.count_nonzero(occ)),
+                      "xyh_cells": int(occ.size), "worst_heading_blocked_frac": max(per_h),
+                      "best_heading_blocked_frac": min(per_h)},
+        "targets": targets,
+        "targets_ok": all(t["ok"] for t in targets),
+        "recommend": {"size_budget_bytes": float(getc(cfg, "size_budget_bytes", 8 * 2 ** 30)),
+                      "resolution": None, "in_core": None, "tau_options": [],
+                      "tau_max": sp.p.tau_max, "tau_applied": sp.p.tau_max,
+                      "tau_auto": isinstance(getc(cfg, "tau_max", "auto"), str),
+                      "tau_reference": 0.5, "tau_pinned_waste": False, "tau_applied_cost": 0.0,
+                      "tau_reason": "the grid is solved whole on the device, so there is no "
+                                    "halo to trade the horizon against"},
+        "dtype": prep.dtype,
+        "elem_bytes": eb,
+        "bytes_per_target": cells * eb,
+        "n_targets": ntg,
+        "bytes_total": cells * eb * ntg,
+        "chunks_per_target": -(-cells // prep.chunk_elements),
+        "controls": sp.nctl,
+        "storage": sp.storage,
+        "gpu_available": mem is not None,
+        "gpu_fits": bool(fits),
+        "gpu_need_gb": need / 1e9,
+        "gpu_free_gb": (mem[0] / 1e9) if mem else 0.0,
+        "out_of_core": {"mode": "incore" if fits or mem is None else "ooc"},
+        "driver": "whole_grid",
+        "grid_balance": dvd / cell_cm if acc > 0 else float("nan"),
+        "dv_distance_cm": dvd,
+        "max_accel_cm_s2": acc,
+        "cell_cm": cell_cm,
+        "cell_cm_s": dv,
+        "runtime": runtime,
     }

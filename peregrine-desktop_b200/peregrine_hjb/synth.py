@@ -36,6 +36,9 @@ WORKLOADS = {
     # the same per-block work, small enough for a profiler capture
     "medium_h8": dict(n=[48, 48, 8, 15, 15, 15], control_set="cube5", dt=0.04, rects=6),
     "large": dict(n=[96, 96, 64, 21, 21, 21], control_set="cube5", dt=0.03, rects=8),
+    # the large workload's planes and controls with 2 headings: the same
+    # per-block work, a few GB on the device, for profiler captures
+    "large_h2": dict(n=[96, 96, 2, 21, 21, 21], control_set="cube5", dt=0.03, rects=8),
 }
 
 

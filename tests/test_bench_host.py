@@ -40,9 +40,29 @@ def test_onchip_model(bench):
     assert abs(out["flops_per_update"] - (2 * (16 * win + 3) + 4)) < 1e-12
 
 
-def test_committed_profile_feeds_the_rooflines(bench):
-    assert os.path.exists(bench.PROFILE_TRAFFIC)
+def test_profile_figures_only_from_the_current_kernel(bench, tmp_path, monkeypatch):
+    """The issue-roofline instruction count and the DRAM traffic come from
+    the committed ncu summary only when it was captured from the kernel
+    source this tree builds; a summary of another version gives None."""
+    prof = tmp_path / "k.md"
+    monkeypatch.setattr(bench, "profile_path", lambda: str(prof))
+    body = "warp_instructions_per_update: 2.5\ntraffic_bytes_per_launch: 1.5e11\n"
+    prof.write_text(f"source_sha256: {bench.kernel_source_sha()}\n" + body)
+    assert bench.profile_current()
+    assert bench.profiled_value("warp_instructions_per_update") == 2.5
+    assert bench.profiled_traffic() == 1.5e11
+    prof.write_text("source_sha256: " + "0" * 64 + "\n" + body)
+    assert not bench.profile_current()
+    assert bench.profiled_value("warp_instructions_per_update") is None
+    assert bench.profiled_traffic() is None
+
+
+def test_committed_profile_is_of_the_current_kernel(bench):
+    """The committed summary of the benchmark workload exists, parses and
+    was captured from the current kernel source."""
+    assert os.path.exists(bench.profile_path()), bench.profile_path()
+    assert bench.profile_current()
     wipu = bench.profiled_value("warp_instructions_per_update")
     traffic = bench.profiled_traffic()
     assert wipu is not None and 1.0 < wipu < 10.0
-    assert traffic is not None and traffic > 2 * 4 * 248_832_000  # at least V in and out
+    assert traffic is not None and traffic > 2 * 4 * 5_462_360_064  # at least V in and out

@@ -46,7 +46,26 @@ def test_plan_reports_the_grid(tmp_path):
     line = [l for l in r.stdout.splitlines() if l.startswith("PLAN ")][0]
     plan = json.loads(line[5:])
     assert plan["n"] == [24, 24, 16, 9, 9, 9] and plan["cells"] == 6718464
-    assert plan["controls"] == 27 and plan["out_of_core"] is False
+    assert plan["controls"] == 27
+    # the keys the wizard reads (wizard/peregrine.py run_plan and its
+    # show_* helpers), with values that follow from the job
+    for k in ("bounds", "resolution", "occupancy", "targets", "targets_ok", "recommend",
+              "bytes_per_target", "bytes_total", "n_targets", "chunks_per_target",
+              "gpu_available", "gpu_fits", "gpu_need_gb", "gpu_free_gb", "out_of_core",
+              "grid_balance", "cell_cm", "cell_cm_s", "max_accel_cm_s2", "runtime"):
+        assert k in plan, k
+    assert plan["bytes_per_target"] == 6718464 * 2 and plan["n_targets"] == 1
+    assert plan["bytes_total"] == plan["bytes_per_target"]
+    assert plan["chunks_per_target"] == 1 and plan["targets_ok"] is True
+    assert plan["targets"][0]["ok"] and plan["targets"][0]["free_seed_cells"] > 0
+    assert plan["out_of_core"]["mode"] in ("incore", "ooc")
+    assert plan["bounds"]["table_min"][0] == 0.0
+    assert abs(plan["bounds"]["table_max"][0] - 365.8) < 1e-3
+    assert 0.0 < plan["occupancy"]["blocked_frac"] < 0.5
+    rt = plan["runtime"]
+    assert rt["unit"] == "sweep" and rt["units"] == 3000
+    assert abs(rt["total_s"] - rt["unit_s"] * rt["units"]) < 1e-9
+    assert plan["resolution"]["pinned_by_n"] is True
 
 
 def test_missing_knee_is_refused(tmp_path):
