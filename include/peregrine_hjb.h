@@ -182,6 +182,25 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m,
                     const pg_params* p, const uint8_t* occ,
                     const float* ctl, int32_t nctl, int32_t storage);
 
+/* Load one x slab of a table: its interior rows [x0, x1) and `halo` rows
+ * either side (clipped to the table), FP32 storage.  Sweeps (pg_sweep,
+ * pg_solve with the row stencil) update the interior only and pass the halo
+ * through; every coordinate, range test and occupancy lookup uses the global
+ * row, so a slab sweep equals the whole-table sweep on its interior as long
+ * as the halo covers one backup's reach in x.  occ is the whole table's; the
+ * context's rows are the global rows [*row0, *row0 + *rows), seeds passed
+ * to pg_solve are indices into that slab's row-major order.  For tables
+ * split over several GPUs (and for the reference's tiles, Tiles.jl:311-340). */
+int pg_load_slab(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                 const uint8_t* occ, const float* ctl, int32_t nctl, int32_t x0, int32_t x1,
+                 int32_t halo, int32_t* row0, int32_t* rows);
+
+/* Rows [r0, r1) of the loaded table (the slab's rows for a slab), FP32
+ * row-major, to or from a host buffer, or a device buffer on the context's
+ * device when on_device is nonzero (for a halo exchange over NCCL). */
+int pg_get_rows(pg_ctx* ctx, int32_t r0, int32_t r1, void* out, int32_t on_device);
+int pg_set_rows(pg_ctx* ctx, int32_t r0, int32_t r1, const void* in, int32_t on_device);
+
 /* Seed and iterate on the loaded problem (solve_value!, Run.jl:1434-1474). */
 int pg_solve(pg_ctx* ctx, const int64_t* tidx, int64_t ntidx, int32_t iters,
              double tol, const pg_solve_opts* opts, pg_solve_result* res,
@@ -315,6 +334,63 @@ int pg_adjoint(pg_ctx* ctx, const float* dl_dv, int32_t dl_dv_on_device,
  * quoted against these.  Any output may be NULL to skip that probe. */
 int pg_measure_peaks(int device, double* smem_gbs, double* l2_gbs,
                      double* fma_tflops);
+
+/* ------------------------------------------------------------------ */
+/* out of core: a table larger than device memory, a tile of x rows at   */
+/* a time (solve_value_ooc!, solver/src/OutOfCore.jl:412-584; tiles and */
+/* halo from the reach, solver/src/Tiles.jl:104-187, 311-315, 446-476).  */
+/* ------------------------------------------------------------------ */
+
+typedef struct pg_ooc_opts {
+    int32_t tile_rows;      /* interior x rows per tile; 0: the most that fit */
+    int32_t halo_rows;      /* x rows loaded each side; 0: the reach plus two */
+    int32_t tile_sweeps;    /* sweeps per tile residency (tile_sweeps, 4)     */
+    int32_t jacobi;         /* 1: each round reads the last round's table (two
+                               host tables; with tile_sweeps = 1 a round is one
+                               whole-table Jacobi sweep); 0: tiles are written
+                               back in place (one host table)                 */
+    int32_t kernel;         /* PG_KERNEL_STENCIL_ROWS or PG_KERNEL_STENCIL_EXACT */
+    int32_t storage;        /* PG_STORE_F32, F16 or BF16: the host table's type */
+    int32_t stop_rule;      /* PG_STOP_MAXNORM (max over a round) or L1_QUIET */
+    int32_t allow_starved_halo; /* 1: accept a halo below the reach (tests)   */
+    int64_t device_budget_bytes; /* 0: free device memory less 2 GiB          */
+    int32_t reserved[4];
+} pg_ooc_opts;
+
+typedef struct pg_ooc_result {
+    int32_t rounds;         /* rounds run (each sweeps every tile tile_sweeps times) */
+    int32_t tiles_per_round;
+    int32_t tile_rows;      /* interior rows per tile                          */
+    int32_t halo_rows;      /* halo rows per side                              */
+    int32_t reach_rows;     /* the largest successor offset in x, in rows      */
+    int32_t reserved;
+    double last_delta;      /* L1 change of the last round / tile_sweeps       */
+    double last_maxnorm;    /* largest single-cell change of the last round    */
+    double kernel_ms;       /* device time of the rounds (compute stream)      */
+    double elapsed_ms;      /* host wall time of the call                      */
+    int64_t h2d_bytes;      /* table bytes moved to the device                 */
+    int64_t d2h_bytes;      /* and back                                        */
+    int64_t launches;       /* sweep kernel launches                           */
+} pg_ooc_result;
+
+void pg_default_ooc_opts(pg_ooc_opts* opts);
+
+/* The largest successor offset in x over every (plane, control) of the plain
+ * scheme, in rows (one backup's reach; a tile or slab halo needs reach + 2,
+ * the rule of solver/src/Tiles.jl:311-315).  Measured on `device`. */
+int pg_reach_rows(int device, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                  const float* ctl, int32_t nctl, int32_t* reach);
+
+/* Solve with the table on the host: V_host holds ncells values of
+ * opts->storage in the table's row-major order and is written in full (the
+ * solve starts from value_cap with the seeds at zero, as solve_value! does).
+ * Runs `rounds` rounds or until the stop rule's measure of a round is <= tol.
+ * The plain scheme only.  A halo below the reach is refused with PG_EINVAL
+ * (the reference refuses a halo that is too small, Run.jl:1688-1691). */
+int pg_solve_ooc(int device, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                 const uint8_t* occ, const int64_t* tidx, int64_t ntidx, const float* ctl,
+                 int32_t nctl, int32_t rounds, double tol, const pg_ooc_opts* opts,
+                 void* V_host, pg_ooc_result* res, pg_progress_cb cb, void* user);
 
 /* ------------------------------------------------------------------ */
 /* self-test probes: the device's own implementations of the           */

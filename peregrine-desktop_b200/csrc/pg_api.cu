@@ -107,6 +107,8 @@ struct pg_ctx {
     float* stage_d = nullptr;  // row-major f32 staging for get/set
     size_t stage_cap = 0;
 
+    bool slab = false;           // loaded as an x slab (pg_load_slab): row stencil only
+
     void free_values() {
         for (int i = 0; i < 2; ++i) {
             if (V[i]) cudaFree(V[i]);
@@ -320,6 +322,9 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
         (esc || !((kernel == PG_KERNEL_STENCIL && (r_ok || b_ok)) ||
                   (kernel == PG_KERNEL_STENCIL_BLEND && b_ok))))
         return fail(PG_EUNSUPPORTED, "Q16 storage is swept by the blend-then-shift kernels only");
+    if (ctx->slab && (esc || kernel == PG_KERNEL_CELLFORM))
+        return fail(PG_EUNSUPPORTED, "a slab is swept by the row stencil (PG_KERNEL_STENCIL_ROWS, "
+                                     "PG_KERNEL_STENCIL_EXACT or PG_KERNEL_STENCIL)");
     if (kernel == PG_KERNEL_STENCIL_BLEND && !esc && !b_ok)
         return fail(PG_EUNSUPPORTED, "the blend-then-shift kernel cannot run this table (its "
                                      "tiling, shared memory, or FP64 storage)");
@@ -334,6 +339,10 @@ int sweep_async(pg_ctx* ctx, int kernel, int32_t phase, bool esc, int16_t* argmi
         e = pg::launch_stencil_b(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
                                  ctx->kp, ctx->order_d, sb, argmin_d, ctx->stream,
                                  &ctx->launches);
+    else if (kernel == PG_KERNEL_STENCIL && ctx->storage == PG_STORE_F64 && ctx->mask_ok &&
+             ctx->kp.btile_x > 0)
+        e = pg::launch_stencil_d(vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d, ctx->kp, sb,
+                                 argmin_d, ctx->stream, &ctx->launches);
     else if ((kernel == PG_KERNEL_STENCIL || kernel == PG_KERNEL_STENCIL_GATHER) && ctx->mask_ok &&
              ctx->gather_ok && ctx->storage != PG_STORE_F64)
         e = pg::launch_stencil_u(ctx->storage, vin, vout, ctx->occ_d, ctx->mask_d, ctx->recs_d,
@@ -501,11 +510,37 @@ int pg_destroy(pg_ctx* ctx) {
     return PG_OK;
 }
 
-int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_params* p,
-                    const uint8_t* occ, const float* ctl, int32_t nctl, int32_t storage) {
+}  // extern "C"
+
+namespace {
+
+// An x slab of a table: interior rows [x0, x1) with `halo` rows either side.
+struct SlabSpec {
+    int32_t x0, x1, halo;
+};
+
+int load_impl(pg_ctx* ctx, const pg_grid6* g_in, const pg_model* m, const pg_params* p,
+              const uint8_t* occ, const float* ctl, int32_t nctl, int32_t storage,
+              const SlabSpec* slab) {
     int rc = check_ctx(ctx, false);
     if (rc) return rc;
-    if (!g || !m || !p || !occ || !ctl) return fail(PG_EINVAL, "null argument");
+    if (!g_in || !m || !p || !occ || !ctl) return fail(PG_EINVAL, "null argument");
+    const pg_grid6* g = g_in;
+    pg_grid6 gl;
+    int32_t xa = 0;
+    if (slab) {
+        const int32_t n1 = g_in->n[0];
+        if (slab->x0 < 0 || slab->x1 > n1 || slab->x0 >= slab->x1 || slab->halo < 0)
+            return fail(PG_EINVAL, "a slab needs 0 <= x0 < x1 <= Nx and halo >= 0");
+        if (storage != PG_STORE_F32)
+            return fail(PG_EUNSUPPORTED, "slabs are swept in FP32 storage");
+        xa = std::max(0, slab->x0 - slab->halo);
+        const int32_t xb = std::min(n1, slab->x1 + slab->halo);
+        if (xb - xa < 2) return fail(PG_EINVAL, "a slab needs at least 2 rows with its halo");
+        gl = *g_in;
+        gl.n[0] = xb - xa;
+        g = &gl;
+    }
     for (int k = 0; k < 6; ++k)
         if (g->n[k] < 2)
             return fail(PG_EINVAL, "every axis needs at least 2 samples (Grid6)");
@@ -532,6 +567,10 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     kp.nplanes = (int64_t)g->n[2] * g->n[3] * g->n[4] * g->n[5];
     kp.ncells = kp.P * kp.nplanes;
     kp.nctl = nctl;
+    kp.xoff = xa;
+    kp.n1g = g_in->n[0];
+    kp.ux0 = slab ? slab->x0 - xa : 0;
+    kp.ux1 = slab ? slab->x1 - xa : g->n[0];
     // Stencil tiling: a block takes whole planes (x rows split only past 4096
     // four-cell segments), and the block size is the multiple of 32 in
     // [96, 256] that leaves the fewest idle threads in the last pass.
@@ -616,7 +655,9 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     rc = ensure_values(ctx, storage);
     if (rc) { ctx->free_problem(); return rc; }
 
-    const int32_t nx = g->n[0], ny = g->n[1], nh = g->n[2];
+    // the whole table's occupancy, also for a slab (its sweep reads it at
+    // global rows)
+    const int32_t nx = g_in->n[0], ny = g->n[1], nh = g->n[2];
     std::vector<uint8_t> occ_hxy((size_t)nx * ny * nh);
     for (int32_t i = 0; i < nx; ++i)
         for (int32_t j = 0; j < ny; ++j)
@@ -663,10 +704,14 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     // fit (the row-order mask is then made a chunk of planes at a time and
     // dropped), else the row-order mask alone; with neither, the row stencil
     // decides per sweep.
-    if (ctx->stencil_ok && storage != PG_STORE_F64) {
+    // FP64 storage keeps the row-order mask and records only: its sweep is
+    // the precision oracle, which takes the FP32 solver's decisions.  A slab
+    // runs the row stencil, which decides every probe per sweep.
+    if (ctx->stencil_ok && !slab) {
         const size_t mb = pg::stencil_mask_bytes(kp), rb = pg::stencil_recs_bytes(kp);
         const size_t gb = (size_t)kp.nplanes * kp.nctl * sizeof(uint16_t);
-        const bool r_able = kp.rtile_x > 0 && kp.nctl <= 0x7fff && r_smem_fits(kp);
+        const bool r_able = storage != PG_STORE_F64 && kp.rtile_x > 0 && kp.nctl <= 0x7fff &&
+                            r_smem_fits(kp);
         const size_t tb = r_able ? pg::stencil_tmask_bytes(kp) : 0;
         const size_t G = (size_t)1 << 30;
         size_t fr = 0, tot = 0;
@@ -690,8 +735,9 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
                                         kp.nplanes, ctx->stream, &ctx->launches);
             if (e != cudaSuccess) return fail(PG_ECUDA, std::string("prep: ") + cudaGetErrorString(e));
             ctx->mask_ok = true;
-            ctx->blend_ok = kp.btile_x > 0 && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
-            ctx->gather_ok = pg::stencil_u_smem_bytes(kp) <= 200 * 1024;
+            ctx->blend_ok = storage != PG_STORE_F64 && kp.btile_x > 0 &&
+                            pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
+            ctx->gather_ok = storage != PG_STORE_F64 && pg::stencil_u_smem_bytes(kp) <= 200 * 1024;
         }
         if ((keep_rows || r_only) && r_able) {
             size_t fr2 = 0, tot2 = 0;
@@ -723,6 +769,68 @@ int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_
     }
     PG_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->loaded = true;
+    ctx->slab = slab != nullptr;
+    return PG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pg_load_problem(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                    const uint8_t* occ, const float* ctl, int32_t nctl, int32_t storage) {
+    return load_impl(ctx, g, m, p, occ, ctl, nctl, storage, nullptr);
+}
+
+int pg_load_slab(pg_ctx* ctx, const pg_grid6* g, const pg_model* m, const pg_params* p,
+                 const uint8_t* occ, const float* ctl, int32_t nctl, int32_t x0, int32_t x1,
+                 int32_t halo, int32_t* row0, int32_t* rows) {
+    const SlabSpec sl{x0, x1, halo};
+    int rc = load_impl(ctx, g, m, p, occ, ctl, nctl, PG_STORE_F32, &sl);
+    if (rc) return rc;
+    if (row0) *row0 = ctx->kp.xoff;
+    if (rows) *rows = ctx->kp.g.n[0];
+    return PG_OK;
+}
+
+int pg_get_rows(pg_ctx* ctx, int32_t r0, int32_t r1, void* out, int32_t on_device) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (!out) return fail(PG_EINVAL, "null argument");
+    if (ctx->storage != PG_STORE_F32) return fail(PG_EUNSUPPORTED, "row copies read FP32 storage");
+    if (r0 < 0 || r1 > ctx->kp.g.n[0] || r1 < r0) return fail(PG_EINVAL, "rows out of range");
+    const size_t bytes = (size_t)(r1 - r0) * (size_t)(ctx->kp.ncells / ctx->kp.g.n[0]) * 4;
+    if (bytes == 0) return PG_OK;
+    void* dst = out;
+    if (!on_device) {
+        rc = ensure_stage(ctx);
+        if (rc) return rc;
+        dst = ctx->stage_d;
+    }
+    PG_CUDA(pg::launch_slab_out(4, ctx->V[ctx->cur], dst, ctx->kp, r0, r1, ctx->stream));
+    if (!on_device)
+        PG_CUDA(cudaMemcpyAsync(out, ctx->stage_d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PG_OK;
+}
+
+int pg_set_rows(pg_ctx* ctx, int32_t r0, int32_t r1, const void* in, int32_t on_device) {
+    int rc = check_ctx(ctx, true);
+    if (rc) return rc;
+    if (!in) return fail(PG_EINVAL, "null argument");
+    if (ctx->storage != PG_STORE_F32) return fail(PG_EUNSUPPORTED, "row copies write FP32 storage");
+    if (r0 < 0 || r1 > ctx->kp.g.n[0] || r1 < r0) return fail(PG_EINVAL, "rows out of range");
+    const size_t bytes = (size_t)(r1 - r0) * (size_t)(ctx->kp.ncells / ctx->kp.g.n[0]) * 4;
+    if (bytes == 0) return PG_OK;
+    const void* src = in;
+    if (!on_device) {
+        rc = ensure_stage(ctx);
+        if (rc) return rc;
+        PG_CUDA(cudaMemcpyAsync(ctx->stage_d, in, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        src = ctx->stage_d;
+    }
+    PG_CUDA(pg::launch_slab_in(4, src, ctx->V[ctx->cur], ctx->kp, ctx->stream, r0, r1));
+    PG_CUDA(cudaStreamSynchronize(ctx->stream));
     return PG_OK;
 }
 
@@ -1147,7 +1255,8 @@ int pg_set_tile_rows(pg_ctx* ctx, int32_t rows) {
     } else {
         kp.btile_x = kp.btiles_x = kp.bblock = 0;
     }
-    ctx->blend_ok = ctx->mask_ok && b_fits && pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
+    ctx->blend_ok = ctx->mask_ok && ctx->storage != PG_STORE_F64 && b_fits &&
+                    pg::stencil_b_smem_bytes(kp) <= 200 * 1024;
     r_tiling(kp, r_fits ? rows : -1);
     return build_r_tables(ctx);
 }

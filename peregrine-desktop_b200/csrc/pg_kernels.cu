@@ -582,6 +582,7 @@ __global__ void __launch_bounds__(kCellThreads)
 #include "pg_stencil_u.cuh"
 #include "pg_stencil_b.cuh"
 #include "pg_stencil_r.cuh"
+#include "pg_stencil_d.cuh"
 #include "pg_adjoint.cuh"
 
 // ---------------------------------------------------------------------------
@@ -1174,6 +1175,46 @@ cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uin
     return cudaErrorInvalidValue;
 }
 
+template <bool ARGMIN>
+static cudaError_t stencil_d_t(const void* Vin, void* Vout, const uint8_t* occ,
+                               const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                               const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                               int64_t* launches) {
+    if (kp.btile_x <= 0 || (int64_t)kp.btile_x * kp.g.n[1] > kBCells * kDThreads ||
+        kp.nsub > kStencilMaxSub)
+        return cudaErrorInvalidValue;
+    KParams kd = kp;
+    kd.tile_x = kp.btile_x;
+    kd.tiles_x = kp.btiles_x;
+    const int64_t blocks = kp.nplanes * kp.btiles_x;
+    if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const size_t smem = stencil_d_smem(kp.btile_x, kp.g.n[1]);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static std::atomic<uint64_t> attr_set{0};
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set.load() & attr_bit)) {
+        cudaError_t e = cudaFuncSetAttribute(k_stencil_d<ARGMIN>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set.fetch_or(attr_bit);
+    }
+    k_stencil_d<ARGMIN><<<(unsigned)blocks, kDThreads, smem, st>>>(
+        (const double*)Vin, (double*)Vout, occ, mask, recs, kd, sb.part_sum, sb.part_max, argmin);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil_d(const void* Vin, void* Vout, const uint8_t* occ,
+                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                             const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                             int64_t* launches) {
+    return argmin ? stencil_d_t<true>(Vin, Vout, occ, mask, recs, kp, sb, argmin, st, launches)
+                  : stencil_d_t<false>(Vin, Vout, occ, mask, recs, kp, sb, argmin, st, launches);
+}
+
 cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, int64_t plane0,
                                  int64_t nplanes, uint32_t* tmask, cudaStream_t st,
                                  int64_t* launches) {
@@ -1279,6 +1320,121 @@ cudaError_t launch_encode(int storage, const void* V, const KParams& kp, int32_t
     return cudaGetLastError();
 }
 
+
+// ---------------------------------------------------------------------------
+// x slabs of the out-of-core driver: a slab's rows between the table's
+// row-major order (the host store) and the device layout, bits unchanged
+// (E = the storage's word: 4 or 2 bytes).  k_slab_in reads every row of the
+// slab; k_slab_out writes the rows [r0, r1) only (row r0 first).  And the
+// per-round residual: the sweep's (L1, max) folded into a running pair.
+// ---------------------------------------------------------------------------
+template <typename E>
+__global__ void k_slab_in(const E* __restrict__ rm, E* __restrict__ V, KParams kp, int32_t row0,
+                          int32_t row1) {
+    const Layout L = make_layout(kp);
+    const int64_t per_row = kp.ncells / L.n[0];
+    const int64_t n = (int64_t)(row1 - row0) * per_row;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = k + (int64_t)row0 * per_row;
+        int32_t i[6];
+        for (int c = 5; c >= 1; --c) { i[c] = (int32_t)(r % L.n[c]); r /= L.n[c]; }
+        i[0] = (int32_t)r;
+        V[L.dev(i[0], i[1], i[2], i[3], i[4], i[5])] = rm[k];
+    }
+}
+
+template <typename E>
+__global__ void k_slab_out(const E* __restrict__ V, E* __restrict__ rm, KParams kp, int32_t row0,
+                           int32_t row1) {
+    const Layout L = make_layout(kp);
+    const int64_t per_row = kp.ncells / L.n[0];
+    const int64_t n = (int64_t)(row1 - row0) * per_row;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = k + (int64_t)row0 * per_row;
+        int32_t i[6];
+        for (int c = 5; c >= 1; --c) { i[c] = (int32_t)(r % L.n[c]); r /= L.n[c]; }
+        i[0] = (int32_t)r;
+        rm[k] = V[L.dev(i[0], i[1], i[2], i[3], i[4], i[5])];
+    }
+}
+
+__global__ void k_accum(const double* __restrict__ red, double* __restrict__ acc) {
+    acc[0] += red[0];
+    acc[1] = fmax(acc[1], red[1]);
+}
+
+cudaError_t launch_slab_in(int elem_bytes, const void* rm, void* V, const KParams& kp,
+                           cudaStream_t st, int32_t row0, int32_t row1) {
+    if (row1 < 0) row1 = kp.g.n[0];
+    if (row0 < 0 || row1 > kp.g.n[0] || row1 < row0) return cudaErrorInvalidValue;
+    const int64_t n = (int64_t)(row1 - row0) * (kp.ncells / kp.g.n[0]);
+    const int b = grid_for(n, 256);
+    if (elem_bytes == 4)
+        k_slab_in<uint32_t><<<b, 256, 0, st>>>((const uint32_t*)rm, (uint32_t*)V, kp, row0, row1);
+    else if (elem_bytes == 2)
+        k_slab_in<uint16_t><<<b, 256, 0, st>>>((const uint16_t*)rm, (uint16_t*)V, kp, row0, row1);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slab_out(int elem_bytes, const void* V, void* rm, const KParams& kp,
+                            int32_t row0, int32_t row1, cudaStream_t st) {
+    if (row0 < 0 || row1 > kp.g.n[0] || row1 < row0) return cudaErrorInvalidValue;
+    const int64_t n = (int64_t)(row1 - row0) * (kp.ncells / kp.g.n[0]);
+    const int b = grid_for(n, 256);
+    if (elem_bytes == 4)
+        k_slab_out<uint32_t><<<b, 256, 0, st>>>((const uint32_t*)V, (uint32_t*)rm, kp, row0, row1);
+    else if (elem_bytes == 2)
+        k_slab_out<uint16_t><<<b, 256, 0, st>>>((const uint16_t*)V, (uint16_t*)rm, kp, row0, row1);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_accum(const double* red, double* acc, cudaStream_t st) {
+    k_accum<<<1, 1, 0, st>>>(red, acc);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// The reach of one backup in x, for the halo of an x slab: the largest
+// |sum of the substep x increments| over every (plane, control), in cells,
+// rounded up (the successor and every swept probe lie between the cell and
+// x + that sum).  One thread per (plane, control), the plain scheme's
+// transition (pg_plane.cuh).
+// ---------------------------------------------------------------------------
+__global__ void k_reach(KParams kp, const float* __restrict__ ctl, int32_t* __restrict__ out) {
+    GridT<float> g;
+    load_grid(g, kp.g);
+    const int64_t total = kp.nplanes * kp.nctl;
+    int32_t best = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pl = i / kp.nctl;
+        const int u = (int)(i - pl * kp.nctl);
+        int64_t q = pl;
+        const int32_t i6 = (int32_t)(q % kp.g.n[5]); q /= kp.g.n[5];
+        const int32_t i5 = (int32_t)(q % kp.g.n[4]); q /= kp.g.n[4];
+        const int32_t i4 = (int32_t)(q % kp.g.n[3]); q /= kp.g.n[3];
+        const int32_t i3 = (int32_t)q;
+        Transition<float> t;
+        transition(kp, g, i3, i4, i5, i6, ctl, u, t);
+        if (!t.ok) continue;
+        const float c = ceilf(fabsf(t.sumx) / g.step[0]);
+        best = max(best, c < 1.0e6f ? (int32_t)c : 1000000);
+    }
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+cudaError_t launch_reach(const KParams& kp, const float* ctl, int32_t* out, cudaStream_t st) {
+    const int64_t total = kp.nplanes * kp.nctl;
+    k_reach<<<grid_for(total, 128), 128, 0, st>>>(kp, ctl, out);
+    return cudaGetLastError();
+}
 
 // ---------------------------------------------------------------------------
 // Self-test probes: the device's own implementations of the reference's

@@ -53,6 +53,12 @@ cudaError_t launch_stencil_r(int storage, const void* Vin, void* Vout, const uin
                              const uint32_t* recs, const uint32_t* tmask, const KParams& kp,
                              const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
                              cudaStream_t st, int64_t* launches);
+// The FP64 precision oracle of the plain sweep: FP32 decisions (mask,
+// records), FP64 value arithmetic and storage; the blend tiling.
+cudaError_t launch_stencil_d(const void* Vin, void* Vout, const uint8_t* occ,
+                             const uint32_t* mask, const uint32_t* recs, const KParams& kp,
+                             const SweepBufs& sb, int16_t* argmin, cudaStream_t st,
+                             int64_t* launches);
 // Tile-order mask of the planes [plane0, plane0 + nplanes) from their row-order
 // words in `mask` (plane plane0 first).
 cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, int64_t plane0,
@@ -89,6 +95,18 @@ cudaError_t launch_adj_grad(const float* V, const double* lam, const int16_t* po
 size_t stencil_u_smem_bytes(const KParams& kp);
 size_t stencil_recs_bytes(const KParams& kp);
 size_t stencil_mask_bytes(const KParams& kp);
+
+// x slabs: row-major store rows <-> device layout (bits unchanged; 4- or
+// 2-byte words), device rows [row0, row1) (slab_in: all rows by default).
+cudaError_t launch_slab_in(int elem_bytes, const void* rm, void* V, const KParams& kp,
+                           cudaStream_t st, int32_t row0 = 0, int32_t row1 = -1);
+cudaError_t launch_slab_out(int elem_bytes, const void* V, void* rm, const KParams& kp,
+                            int32_t row0, int32_t row1, cudaStream_t st);
+// acc[0] += red[0]; acc[1] = max(acc[1], red[1]) (one thread)
+cudaError_t launch_accum(const double* red, double* acc, cudaStream_t st);
+// The largest successor reach in x over every (plane, control), in cells
+// (atomic max into *out, which the caller zeroes).
+cudaError_t launch_reach(const KParams& kp, const float* ctl, int32_t* out, cudaStream_t st);
 
 cudaError_t launch_probe_step(const pg_model& m, int32_t rk2, const float* states,
                               const float* controls, const float* dt, const int32_t* nsub,

@@ -147,6 +147,10 @@ int pg_sweep_noalloc(const pg_grid6* g, const pg_model* m, const pg_params* p,
     kp.ncells = ncells;
     kp.nctl = nctl;
     kp.phase = phase;
+    kp.xoff = 0;
+    kp.n1g = g->n[0];
+    kp.ux0 = 0;
+    kp.ux1 = g->n[0];
     pg::SweepBufs sb{scratch, scratch + kMaxParts, kMaxParts, scratch + 2 * kMaxParts};
 
     cudaStream_t st = (cudaStream_t)stream;

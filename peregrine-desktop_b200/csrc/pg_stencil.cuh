@@ -171,18 +171,23 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
 
-    // ---- phase B: R consecutive cells of one row per thread
+    // ---- phase B: R consecutive cells of one row per thread.  Rows are the
+    // device table's (a slab of the global table when kp.xoff > 0 or
+    // kp.n1g > n1); every coordinate, range test and occupancy lookup uses
+    // the global row, so a slab sweeps exactly as the whole table does.
     const int32_t n1 = L.n[0], n2 = L.n[1];
+    const int32_t n1g = kp.n1g, xoff = kp.xoff;
     const int32_t x0 = xt * kp.tile_x;
     const int32_t x1 = min(x0 + kp.tile_x, n1);
     const int32_t spr = (n2 + R - 1) / R;  // segments per row
     const int32_t nseg = (x1 - x0) * spr;
     const T lo0 = g.lo[0], lo1 = g.lo[1], st0 = g.step[0], st1 = g.step[1];
     const T rs0 = (T)1 / st0, rs1 = (T)1 / st1;
-    const T hx = (T)(n1 - 1), hy = (T)(n2 - 1);
+    const T hx = (T)(n1g - 1), hy = (T)(n2 - 1);
     const int64_t P = L.P;
     const S* __restrict__ Vp0 = Vin + pl * P;
-    const uint8_t* occ_h = occ + (int64_t)i3 * n1 * n2;
+    // the global occupancy (Nh x n1g x n2), this plane's heading, the slab's rows
+    const uint8_t* occ_h = occ + ((int64_t)i3 * n1g + xoff) * n2;
     T ap[kStencilMaxChk];
 #pragma unroll
     for (int sc = 0; sc < kStencilMaxChk; ++sc) ap[sc] = R_::div((T)(sc + 1), (T)(nchk > 0 ? nchk : 1));
@@ -191,6 +196,16 @@ __global__ void __launch_bounds__(256)
     for (int seg = threadIdx.x; seg < nseg; seg += blockDim.x) {
         const int32_t i1 = x0 + seg / spr;
         const int32_t j0 = (seg - (i1 - x0) * spr) * R;
+        if (i1 < kp.ux0 || i1 >= kp.ux1) {
+            // a halo row of a slab: passed through unchanged
+            for (int r = 0; r < R; ++r) {
+                const int32_t j = j0 + r;
+                if (j >= n2) break;
+                const int64_t didx = pl * P + (int64_t)i1 * n2 + j;
+                Vout[didx] = Vin[didx];
+            }
+            continue;
+        }
         T old[R], y[R], best[R];
         int bk[R];
         bool live[R];  // inside the row and not blocked
@@ -207,7 +222,7 @@ __global__ void __launch_bounds__(256)
             bk[r] = 0x7fffffff;
         }
         if (any) {
-            const T x = axisvalue(g, 0, i1);
+            const T x = axisvalue(g, 0, xoff + i1);
             for (int uu = 0; uu < nctl; ++uu) {
                 const int u = ord[uu];
                 const T* rec = rt + (size_t)u * RL.NT;
@@ -239,8 +254,12 @@ __global__ void __launch_bounds__(256)
                     if (xok) {
                         const T b1 = R_::floor_(f1);
                         const T t1 = R_::sub(f1, b1);
-                        const int32_t j1 = (int32_t)b1;
-                        const int32_t j1p = min(j1 + 1, n1 - 1);
+                        // the successor's rows, global, then in the slab (a
+                        // halo as wide as the reach keeps them inside it; the
+                        // clamp only keeps a starved halo's reads in bounds)
+                        const int32_t j1g = (int32_t)b1;
+                        const int32_t j1 = min(max(j1g - xoff, 0), n1 - 1);
+                        const int32_t j1p = min(max(min(j1g + 1, n1g - 1) - xoff, 0), n1 - 1);
                         // y part, per cell
                         T t2[R];
                         int32_t j2[R];
@@ -253,7 +272,7 @@ __global__ void __launch_bounds__(256)
                         int64_t orow[kStencilMaxChk];
 #pragma unroll
                         for (int sc = 0; sc < kStencilMaxChk; ++sc)
-                            orow[sc] = sc < nchk ? ((int64_t)irec[RL.ck(sc)] * n1 + ci[sc]) * n2 : 0;
+                            orow[sc] = sc < nchk ? ((int64_t)irec[RL.ck(sc)] * n1g + ci[sc]) * n2 : 0;
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
                             ok[r] = live[r];

@@ -29,7 +29,7 @@
 // reads instead of 64 shifted gathers.  FP32 arithmetic with FMAs; the
 // result differs from the reference's by the rounding order of the
 // interpolation sum, never in a corner, a fraction or an admissibility
-// decision (those are the mask's).  Each control's 288-byte record is
+// decision (those are the mask's).  Each control's 304-byte record is
 // copied into shared memory with cp.async one control ahead, so its latency
 // hides behind the previous control's work and the block's shared memory
 // (and with it the L1 capacity left for the corner planes) stays small.

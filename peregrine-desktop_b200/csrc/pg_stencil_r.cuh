@@ -50,6 +50,12 @@ __device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
     return d;
 }
+// a - b per lane, IEEE round to nearest (sub.rn.f32x2)
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
 
 // Controls of a plane in group order: entry = control | kGroupFirst on the
 // first control of a group.
@@ -187,15 +193,25 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
 }
 
 // Shared memory of one k_stencil_r block of `threads` threads (a multiple of
-// 32) with KR cells per thread: the plane's group order; per control its
-// record's weights, tau, offsets, admissibility and substeps (24 words) and
-// its substep position increments (x, then y, each rounded up to 4 words);
-// its mask words (one per warp and cell slot: the tile's words, zero beyond
-// them) and its successor entries (the tile's rows, then every column); and
-// two padded window buffers with room for every thread's KR window slots
-// (slots past the window land in scratch rows).
-constexpr int kRWt = 24;  // w[16], tau, tx, ty, -, ox, oy, ok, nsub
-__host__ __device__ inline int32_t stencil_r_ninc(int nsub) { return (nsub + 3) & ~3; }
+// 32) with KR cells per thread: the plane's group order; per control a
+// parameter area of kRWt + 2 NI words -- staged as its record's weights,
+// tau, offsets, admissibility and substeps (24 words) and its substep
+// position increments (x, then y, NI words each), and once the successor
+// entries are made, rewritten as the 16 weights each duplicated into an
+// FP32 pair (32 words) and the 8 parameter words; its mask words (one per
+// warp and cell slot, a warp's KR words together, zero past the tile's);
+// its successor entries (the tile's rows, then every column); and two
+// padded window buffers with room for every thread's KR window slots (slots
+// past the window land in scratch rows).
+constexpr int kRWt = 24;  // as staged: w[16], tau, tx, ty, -, ox, oy, ok, nsub
+// as rewritten: (w, w) pairs in words 0-31, then tau, tx, ty, -, ox, oy, ok, nsub
+constexpr int kRTau = 32, kROx = 36, kROk = 38;
+// x and y increments per control: at least 8 each, so that the parameter
+// area holds the rewritten 40 words
+__host__ __device__ inline int32_t stencil_r_ninc(int nsub) {
+    const int32_t n = (nsub + 3) & ~3;
+    return n > 8 ? n : 8;
+}
 __host__ __device__ inline int32_t stencil_r_window_rows(int tile_x, int n2, int threads, int kr) {
     const int32_t slots = (kr * threads + n2 - 1) / n2;
     return slots > tile_x + 3 ? slots : tile_x + 3;
@@ -231,10 +247,10 @@ __device__ __forceinline__ void stencil_r_item(
     const int32_t TS = tile_mask_stride(TX, n2);  // mask words per control in the tile mask
     const int32_t NI = stencil_r_ninc(kp.nsub);   // increments per axis in shared memory
     const int32_t ecs = TX + n2;  // successor entries per control
+    const int32_t RW = kRWt + 2 * NI;    // parameter words per control
     uint16_t* ord = reinterpret_cast<uint16_t*>(smem_raw);
-    float* wt = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));  // [nctl][kRWt]
-    float* incs = wt + nctl * kRWt;                                   // [nctl][2 NI]
-    uint32_t* msk = reinterpret_cast<uint32_t*>(incs + nctl * 2 * NI);  // [nctl][MWS]
+    float* wt = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));  // [nctl][RW]
+    uint32_t* msk = reinterpret_cast<uint32_t*>(wt + nctl * RW);    // [nctl][MWS]
     // [nctl][ecs]: TX rows (window offset, x fraction), n2 columns (column,
     // y fraction)
     int2* ent = reinterpret_cast<int2*>(msk + nctl * MWS);
@@ -264,7 +280,7 @@ __device__ __forceinline__ void stencil_r_item(
     for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
     for (int i = tid; i < nctl * 6; i += T) {
         const int u = i / 6, c = i - u * 6;
-        cp_async16(wt + u * kRWt + 4 * c, prec + (size_t)u * kURec + (c < 5 ? 4 * c : kUNT + 16));
+        cp_async16(wt + u * RW + 4 * c, prec + (size_t)u * kURec + (c < 5 ? 4 * c : kUNT + 16));
     }
     {
         const int32_t pieces = NI / 2;  // 16-byte pieces per control: NI/4 for x, NI/4 for y
@@ -272,20 +288,22 @@ __device__ __forceinline__ void stencil_r_item(
             const int u = i / pieces, c = i - u * pieces;
             const int32_t half = NI / 4;
             const int32_t src = c < half ? kUInc + 4 * c : kUInc + kStencilMaxSub + 4 * (c - half);
-            cp_async16(incs + u * 2 * NI + 4 * c, prec + (size_t)u * kURec + src);
+            cp_async16(wt + u * RW + kRWt + 4 * c, prec + (size_t)u * kURec + src);
         }
     }
     {
+        // tile word tw = q * mwq + w (cell slot q, warp w) lands at w * KR + q,
+        // so that a warp's KR words are one vector; words past the tile's are 0
         const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * TS;
-        const int32_t p4 = TS / 4;
-        for (int i = tid; i < nctl * p4; i += T) {
-            const int u = i / p4, c = i - u * p4;
-            cp_async16(msk + u * MWS + 4 * c, src + (size_t)u * TS + 4 * c);
+        for (int i = tid; i < nctl * TS; i += T) {
+            const int u = i / TS, tw = i - u * TS;
+            const int32_t q = tw / mwq, w = tw - q * mwq;
+            cp_async4(msk + u * MWS + w * KR + q, src + (size_t)u * TS + tw);
         }
-        const int32_t zw = MWS - TS;
-        for (int i = tid; i < nctl * zw; i += T) {
-            const int u = i / zw;
-            msk[u * MWS + TS + (i - u * zw)] = 0u;
+        for (int i = tid; i < nctl * MWS; i += T) {
+            const int u = i / MWS, r = i - u * MWS;
+            const int32_t w = r / KR, q = r - w * KR;
+            if (q * mwq + w >= TS) msk[i] = 0u;
         }
     }
     cp_async_commit();
@@ -318,9 +336,8 @@ __device__ __forceinline__ void stencil_r_item(
         wsb[k] = a * SB + j;
         if (j == n2 - 1) wlast |= 1u << k;
     }
-    // mask word of cell slot q in a control's words; its bit is the lane
-    const int32_t mw0 = tid >> 5;
-    const int32_t nq = (ncell + T - 1) / T;  // cell slots in use
+    // the warp's mask words in a control's words; its bit is the lane
+    const int32_t mw0 = (tid >> 5) * KR;
     const uint32_t lane = (uint32_t)tid & 31u;
     cp_async_wait_all();
     __syncthreads();
@@ -332,18 +349,35 @@ __device__ __forceinline__ void stencil_r_item(
     for (int32_t i = tid; i < nctl * ecs; i += T) {
         const int u = i / ecs;
         const int32_t k = i - u * ecs;
-        if (__float_as_uint(wt[u * kRWt + 22]) == 0u || (k >= nr && k < TX)) continue;
+        if (__float_as_uint(wt[u * RW + 22]) == 0u || (k >= nr && k < TX)) continue;
         const bool row = k < TX;
         int32_t li;
         float t;
-        succ_li_t(kp.g, incs + u * 2 * NI + (row ? 0 : NI), kp.nsub, row,
+        succ_li_t(kp.g, wt + u * RW + kRWt + (row ? 0 : NI), kp.nsub, row,
                   row ? x0 + k : k - TX, n1, n2, &li, &t);
         if (row) {
-            const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 20]) - 1;
+            const int32_t wbase = x0 + __float_as_int(wt[u * RW + 20]) - 1;
             ent[i] = make_int2(min(max(li - wbase, 0), nr + 1) * SB, __float_as_int(t));
         } else {
             ent[i] = make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
         }
+    }
+    __syncthreads();
+    // the increments are spent: rewrite each control's parameter area as
+    // its weights duplicated into FP32 pairs for the packed blend, then the
+    // eight parameter words (each thread its own controls, so no barrier
+    // between reading and writing one)
+    for (int u = tid; u < nctl; u += T) {
+        float* a = wt + u * RW;
+        float w[16], par[8];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) w[c] = a[c];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) par[c] = a[16 + c];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) { a[2 * c] = w[c]; a[2 * c + 1] = w[c]; }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a[kRTau + c] = par[c];
     }
     __syncthreads();
 
@@ -353,7 +387,7 @@ __device__ __forceinline__ void stencil_r_item(
     // record, rows from its x offset
     auto load_group = [&](int uu) {
         const int u = ord[uu] & 0x7fff;
-        const int32_t wbase = x0 + __float_as_int(wt[u * kRWt + 20]) - 1;
+        const int32_t wbase = x0 + __float_as_int(wt[u * RW + kROx]) - 1;
         const uint32_t* rec = prec + (size_t)u * kURec;
         const S* base[KR];
 #pragma unroll
@@ -372,13 +406,13 @@ __device__ __forceinline__ void stencil_r_item(
     };
     // the first control starts a group; inadmissible controls come last and
     // their records' corner planes are never read
-    if (__float_as_uint(wt[(ord[0] & 0x7fff) * kRWt + 22]) != 0u) load_group(0);
+    if (__float_as_uint(wt[(ord[0] & 0x7fff) * RW + kROk]) != 0u) load_group(0);
     int buf = 0;
     for (int uu = 0; uu < nctl; ++uu) {
         const uint32_t ent_u = ord[uu];
         const int u = (int)(ent_u & 0x7fffu);
-        const float* wu = wt + u * kRWt;
-        if (__float_as_uint(wu[22]) == 0u) {
+        const float* wu = wt + u * RW;
+        if (__float_as_uint(wu[kROk]) == 0u) {
             // no cell of the plane admits this control (block-uniform)
             if constexpr (ARGMIN) {
 #pragma unroll
@@ -397,15 +431,15 @@ __device__ __forceinline__ void stencil_r_item(
             for (int k = 0; k < KR / 2; ++k) acc2[k] = 0ull;
 #pragma unroll
             for (int c4 = 0; c4 < 4; ++c4) {
-                const float4 w = reinterpret_cast<const float4*>(wu)[c4];
-                const uint64_t wx = pk2(w.x, w.x), wy = pk2(w.y, w.y), wz = pk2(w.z, w.z),
-                               ww = pk2(w.w, w.w);
+                // (w, w) pairs of corners 4 c4 .. 4 c4 + 3
+                const ulonglong2 wa = reinterpret_cast<const ulonglong2*>(wu)[2 * c4];
+                const ulonglong2 wb = reinterpret_cast<const ulonglong2*>(wu)[2 * c4 + 1];
 #pragma unroll
                 for (int k = 0; k < KR / 2; ++k) {
-                    acc2[k] = fma2(wx, cv[k][4 * c4 + 0], acc2[k]);
-                    acc2[k] = fma2(wy, cv[k][4 * c4 + 1], acc2[k]);
-                    acc2[k] = fma2(wz, cv[k][4 * c4 + 2], acc2[k]);
-                    acc2[k] = fma2(ww, cv[k][4 * c4 + 3], acc2[k]);
+                    acc2[k] = fma2(wa.x, cv[k][4 * c4 + 0], acc2[k]);
+                    acc2[k] = fma2(wa.y, cv[k][4 * c4 + 1], acc2[k]);
+                    acc2[k] = fma2(wb.x, cv[k][4 * c4 + 2], acc2[k]);
+                    acc2[k] = fma2(wb.y, cv[k][4 * c4 + 3], acc2[k]);
                 }
             }
             float acc[KR];
@@ -421,32 +455,46 @@ __device__ __forceinline__ void stencil_r_item(
         // the corner values are free now: if the next control starts a new
         // group, its loads fly during this control's barrier and phase 2
         if (uu + 1 < nctl && (ord[uu + 1] & kGroupFirst) &&
-            __float_as_uint(wt[(ord[uu + 1] & 0x7fff) * kRWt + 22]) != 0u)
+            __float_as_uint(wt[(ord[uu + 1] & 0x7fff) * RW + kROk]) != 0u)
             load_group(uu + 1);
         __syncthreads();
 
         // phase 2: shift, admissibility, tau, min -- computed for every cell
         // slot (entries are clamped into the window, dead slots read cell
-        // (0, 0)), kept where the cell is free and the control admissible
-        const float tau = wu[16];
+        // (0, 0)), kept where the control is admissible.  The mask has no
+        // bit for an occupied cell or a slot past the tile, so it alone
+        // decides; the bilinear step takes the two row lerps as one packed
+        // FMA (the same IEEE operations per lane as k_stencil_b's).
+        const float tau = wu[kRTau];
         const int2* ri = ent + (size_t)u * ecs;
         const int2* ci = ri + TX;
-        const uint32_t* mu = msk + u * MWS + mw0;
+        uint32_t mw[KR];  // the warp's mask words of this control, one vector load
+        {
+            const uint32_t* mu = msk + u * MWS + mw0;
+            if constexpr (KR == 4) {
+                const uint4 m4 = *reinterpret_cast<const uint4*>(mu);
+                mw[0] = m4.x; mw[1] = m4.y; mw[2] = m4.z; mw[3] = m4.w;
+            } else {
+#pragma unroll
+                for (int q = 0; q < KR; ++q) mw[q] = mu[q];
+            }
+        }
 #pragma unroll
         for (int q = 0; q < KR; ++q) {
-            if (q >= nq) break;  // block-uniform: slots no thread of the tile uses
+            // warp-uniform: slots no lane of the warp has a cell in
+            if ((tid & ~31) + q * T >= ncell) break;
             const int32_t a = caj[q] >> 16, j = caj[q] & 0xffff;
-            const bool adm = ((live >> q) & (mu[q * mwq] >> lane)) & 1u;
+            const bool adm = (mw[q] >> lane) & 1u;
             const int2 rr = ri[a];
             const int2 cc = ci[j];
             const float tx = __int_as_float(rr.y), ty = __int_as_float(cc.y);
             const float* p = B + rr.x + cc.x;
-            const float v00 = p[0], v01 = p[1], v10 = p[SB], v11 = p[SB + 1];
-            const float m0 = fmaf(tx, v10 - v00, v00);
-            const float m1 = fmaf(tx, v11 - v01, v01);
+            const uint64_t lo = pk2(p[0], p[1]), hi = pk2(p[SB], p[SB + 1]);
+            float m0, m1;  // v0c + tx * (v1c - v0c) for columns c = 0, 1
+            upk2(fma2(pk2(tx, tx), sub2(hi, lo), lo), m0, m1);
             const float val = fmaf(ty, m1 - m0, m0);
-            const float cvl = adm ? fminf(tau + fminf(val, cap), cap) : cap;
             if constexpr (ARGMIN) {
+                const float cvl = adm ? fminf(tau + fminf(val, cap), cap) : cap;
                 // equal values go to the lower table index, which is what
                 // the reference's strict < in table order keeps
                 if (cvl < best[q] || (cvl == best[q] && u < bk[q])) {
@@ -454,7 +502,9 @@ __device__ __forceinline__ void stencil_r_item(
                     bk[q] = u;
                 }
             } else {
-                best[q] = fminf(best[q], cvl);
+                // best <= cap throughout, so min(best, min(tau + min(val,
+                // cap), cap)) is min(best, tau + val) for finite values
+                if (adm) best[q] = fminf(best[q], tau + val);
             }
         }
     }

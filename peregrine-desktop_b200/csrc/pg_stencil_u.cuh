@@ -26,17 +26,20 @@ constexpr int kURX = 2;  // rows per thread
 // Mask words per (plane, control, row): ceil(Ny / 32).
 __host__ __device__ inline int32_t mask_words(int32_t n2) { return (n2 + 31) / 32; }
 
-// Record per (plane, control), 72 words, 16-byte aligned:
+// Record per (plane, control), 76 words, 16-byte aligned:
 //   float: w[16] (the (h, v)-corner weights), tau, tx, ty, -
 //   int:   plane[16], ox, oy, ok, nsub
 //   float: incx[16], incy[16] (the field-frame position increment of each
 //          substep, which the reference adds to x and y one at a time)
-// Every vector load on a record is aligned to its size: the record is 288
+//   float: tt[4], the successor's (h, vx, vy, w) fractions the weights are
+//          products of (the FP64 sweep forms its weights from them)
+// Every vector load on a record is aligned to its size: the record is 304
 // bytes, (tau, tx, ty, -) sits at byte 64 and (ox, oy) at byte 144.
 constexpr int kUNT = 20;
 constexpr int kUNI = 20;
 constexpr int kUInc = 40;
-constexpr int kURec = kUInc + 2 * kStencilMaxSub;
+constexpr int kUTT = kUInc + 2 * kStencilMaxSub;
+constexpr int kURec = kUTT + 4;
 
 __host__ __device__ inline size_t stencil_u_smem(int nctl) {
     return (size_t)nctl * (kURec * 4 + 4) + 64;
@@ -111,6 +114,7 @@ __global__ void __launch_bounds__(256)
         rec[kUNT + 17] = (uint32_t)(t.ok ? (int32_t)fy : 0);
         rec[kUNT + 18] = t.ok ? 1u : 0u;
         rec[kUNT + 19] = (uint32_t)nsub;
+        for (int k = 0; k < 4; ++k) rec[kUTT + k] = __float_as_uint(t.ok ? t.tt[k] : 0.0f);
         for (int k = 0; k < kStencilMaxSub; ++k) {
             rec[kUInc + k] = __float_as_uint(t.ok && k < nsub ? t.incx[k] : 0.0f);
             rec[kUInc + kStencilMaxSub + k] = __float_as_uint(t.ok && k < nsub ? t.incy[k] : 0.0f);

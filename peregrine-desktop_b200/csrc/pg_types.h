@@ -56,6 +56,11 @@ struct KParams {
     int32_t relax;    // 0: V' = min(V, T V), the reference's update; 1: V' = T V except
                       // where V = 0 (target cells, which stay pinned)
     int32_t phase;
+    // x slabs (the row stencil only): the device table holds the global rows
+    // [xoff, xoff + g.n[0]) of a table of n1g rows; rows [ux0, ux1) of the
+    // slab are swept, the others (the halo) pass through unchanged.  Whole
+    // tables: xoff = 0, n1g = g.n[0], [ux0, ux1) = [0, g.n[0]).
+    int32_t xoff, n1g, ux0, ux1;
 };
 
 // Per-sweep reduction buffers: one partial per block, reduced in a fixed

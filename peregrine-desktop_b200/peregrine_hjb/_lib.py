@@ -35,7 +35,9 @@ EXPORTS = (
     "pg_sweep", "pg_escape_sweep", "pg_solve_escape", "pg_encode", "pg_time_sweeps",
     "pg_launch_count", "pg_set_tile_rows", "pg_batch_create", "pg_batch_destroy",
     "pg_batch_add", "pg_batch_solve", "pg_batch_table", "pg_adjoint", "pg_measure_peaks",
-    "pg_sweep_noalloc", "pg_set_wait_timeout", "pg_probe_step", "pg_probe_traction_gain", "pg_probe_interp",
+    "pg_sweep_noalloc", "pg_set_wait_timeout", "pg_default_ooc_opts", "pg_solve_ooc",
+    "pg_reach_rows", "pg_load_slab", "pg_get_rows", "pg_set_rows",
+    "pg_probe_step", "pg_probe_traction_gain", "pg_probe_interp",
 )
 
 
@@ -91,6 +93,21 @@ class AdjointResult(C.Structure):
                 ("kernel_ms", C.c_double)]
 
 
+class OocOpts(C.Structure):
+    _fields_ = [("tile_rows", C.c_int32), ("halo_rows", C.c_int32), ("tile_sweeps", C.c_int32),
+                ("jacobi", C.c_int32), ("kernel", C.c_int32), ("storage", C.c_int32),
+                ("stop_rule", C.c_int32), ("allow_starved_halo", C.c_int32),
+                ("device_budget_bytes", C.c_int64), ("reserved", C.c_int32 * 4)]
+
+
+class OocResult(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("tiles_per_round", C.c_int32), ("tile_rows", C.c_int32),
+                ("halo_rows", C.c_int32), ("reach_rows", C.c_int32), ("reserved", C.c_int32),
+                ("last_delta", C.c_double), ("last_maxnorm", C.c_double),
+                ("kernel_ms", C.c_double), ("elapsed_ms", C.c_double),
+                ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("launches", C.c_int64)]
+
+
 PROGRESS_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_double, C.c_double)
 
 _lib = None
@@ -141,6 +158,14 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "pg_sweep_noalloc": (C.c_int, [P(Grid6), P(Model), P(Params), vp, vp, i32, vp, vp, i32,
                                        vp, P(f64), P(f64)]),
         "pg_set_wait_timeout": (C.c_int, [vp, f64]),
+        "pg_default_ooc_opts": (None, [P(OocOpts)]),
+        "pg_reach_rows": (C.c_int, [C.c_int, P(Grid6), P(Model), P(Params), vp, i32, P(i32)]),
+        "pg_load_slab": (C.c_int, [vp, P(Grid6), P(Model), P(Params), vp, vp, i32, i32, i32, i32,
+                                   P(i32), P(i32)]),
+        "pg_get_rows": (C.c_int, [vp, i32, i32, vp, i32]),
+        "pg_set_rows": (C.c_int, [vp, i32, i32, vp, i32]),
+        "pg_solve_ooc": (C.c_int, [C.c_int, P(Grid6), P(Model), P(Params), vp, vp, i64, vp, i32,
+                                   i32, f64, P(OocOpts), vp, P(OocResult), PROGRESS_CB, vp]),
         "pg_probe_step": (C.c_int, [C.c_int, P(Model), i32, vp, vp, vp, vp, i64, vp]),
         "pg_probe_traction_gain": (C.c_int, [C.c_int, vp, C.c_float, i64, vp]),
         "pg_probe_interp": (C.c_int, [vp, vp, i64, i32, i32, i32, C.c_float, vp, vp]),
@@ -303,6 +328,39 @@ class Context:
         _check(self._lib.pg_launch_count(self._h, C.byref(n)))
         return n.value
 
+    def load_slab(self, grid: Grid6, model: Model, params: Params, occ: np.ndarray,
+                  ctl: np.ndarray, x0: int, x1: int, halo: int):
+        """pg_load_slab: rows [x0, x1) of the table with `halo` rows either
+        side; returns (first global row, rows held)."""
+        occ = np.ascontiguousarray(occ, dtype=np.uint8)
+        ctl = np.ascontiguousarray(ctl, dtype=np.float32)
+        r0, nr = C.c_int32(), C.c_int32()
+        _check(self._lib.pg_load_slab(self._h, C.byref(grid), C.byref(model), C.byref(params),
+                                      _ptr(occ), _ptr(ctl), ctl.size // 3, int(x0), int(x1),
+                                      int(halo), C.byref(r0), C.byref(nr)))
+        per = 1
+        for k in range(1, 6):
+            per *= int(grid.n[k])
+        self.ncells = per * nr.value
+        self.nctl = ctl.size // 3
+        self._cap = float(params.cap)
+        self._keep = (occ, ctl)
+        self.row_cells = per
+        return r0.value, nr.value
+
+    def get_rows(self, r0: int, r1: int, out=None, on_device: bool = False):
+        """Rows [r0, r1) (FP32 row-major): into `out` (a numpy array, or with
+        on_device a device pointer / tensor data_ptr)."""
+        if out is None:
+            out = np.empty((r1 - r0) * self.row_cells, np.float32)
+        p = out if on_device else _ptr(out)
+        _check(self._lib.pg_get_rows(self._h, int(r0), int(r1), p, int(on_device)))
+        return out
+
+    def set_rows(self, r0: int, r1: int, src, on_device: bool = False) -> None:
+        p = src if on_device else _ptr(np.ascontiguousarray(src, np.float32))
+        _check(self._lib.pg_set_rows(self._h, int(r0), int(r1), p, int(on_device)))
+
     def set_wait_timeout(self, seconds: float) -> None:
         """Limit each wait for a sweep (0 = no limit); a sweep that outlasts it
         makes the solve raise PeregrineError with code PG_ETIMEOUT."""
@@ -320,6 +378,50 @@ class Context:
         _check(self._lib.pg_probe_interp(self._h, _ptr(st), n, int(kuhn), int(nearest),
                                          int(vclamp), cap, _ptr(out), _ptr(gr)))
         return (out, gr) if grads else out
+
+
+def ooc_opts(**kw) -> OocOpts:
+    lib = load_library()
+    o = OocOpts()
+    lib.pg_default_ooc_opts(C.byref(o))
+    for k, v in kw.items():
+        if k == "storage" and isinstance(v, str):
+            v = STORAGES[v]
+        setattr(o, k, int(v))
+    return o
+
+
+def solve_ooc(grid: Grid6, model: Model, params: Params, occ: np.ndarray, tidx: np.ndarray,
+              ctl: np.ndarray, rounds: int, tol: float, opts: OocOpts | None = None,
+              progress=None, device: int = 0, out: np.ndarray | None = None):
+    """pg_solve_ooc: the table solved a tile of x rows at a time with the
+    table on the host; returns (V row-major in the store's type, result)."""
+    lib = load_library()
+    o = opts if opts is not None else ooc_opts()
+    n = 1
+    for k in range(6):
+        n *= int(grid.n[k])
+    dt = {STORE_F32: np.float32, STORE_F16: np.float16, STORE_BF16: np.uint16}[o.storage]
+    V = out if out is not None else np.empty(n, dtype=dt)
+    occ = np.ascontiguousarray(occ, np.uint8)
+    tidx = np.ascontiguousarray(tidx, np.int64)
+    ctl = np.ascontiguousarray(ctl, np.float32)
+    res = OocResult()
+    _check(lib.pg_solve_ooc(int(device), C.byref(grid), C.byref(model), C.byref(params),
+                            _ptr(occ), _ptr(tidx), tidx.size, _ptr(ctl), ctl.size // 3,
+                            int(rounds), float(tol), C.byref(o), _ptr(V), C.byref(res),
+                            _wrap_cb(progress), None))
+    return V, res
+
+
+def reach_rows(grid: Grid6, model: Model, params: Params, ctl: np.ndarray, device: int = 0) -> int:
+    """pg_reach_rows: one backup's largest x offset, in rows."""
+    lib = load_library()
+    ctl = np.ascontiguousarray(ctl, np.float32)
+    r = C.c_int32()
+    _check(lib.pg_reach_rows(int(device), C.byref(grid), C.byref(model), C.byref(params), _ptr(ctl),
+                             ctl.size // 3, C.byref(r)))
+    return r.value
 
 
 def probe_step(model: Model, states, controls, dt, nsub, rk2=True, device: int = 0):

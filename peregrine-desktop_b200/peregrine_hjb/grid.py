@@ -88,9 +88,11 @@ class Grid6:
         return g
 
     def span_max(self, k: int) -> float:
-        """Manifest `grid.max` (Run.jl:2008)."""
+        """Manifest `grid.max` (Run.jl:2008): lo + step * (n or n - 1), each
+        operation in Float32 as the reference's Grid6 fields are, then
+        widened."""
         m = self.n[k] if k == 2 else self.n[k] - 1
-        return float(self.lo[k]) + float(self.step[k]) * m
+        return float(f32(self.lo[k] + f32(self.step[k] * f32(m))))
 
 
 def axis_samples(span: float, cell: float):

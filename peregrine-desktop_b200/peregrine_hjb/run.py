@@ -178,8 +178,42 @@ def check_targets(prep, occ):
                          "nothing and the whole table would come out unreachable:\n" + "\n".join(bad))
 
 
-def run_solve(cfg, device: int = 0) -> dict:
-    """run_solve (Run.jl:1539-2131) on the GPU."""
+def dist_ranks():
+    """(rank, world, local rank) of this process.  Under a launcher that sets
+    WORLD_SIZE > 1 (torchrun) the process group is initialised here: NCCL
+    when every rank has its own GPU, gloo otherwise (the ranks exchange only
+    small records, never tables)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return 0, 1, 0
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not dist.is_initialized():
+        ngpu = torch.cuda.device_count() if torch.cuda.is_available() else 0
+        backend = "nccl" if ngpu >= world else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return dist.get_rank(), dist.get_world_size(), local
+
+
+def run_solve(cfg, device: int | None = None) -> dict:
+    """run_solve (Run.jl:1539-2131) on the GPU.  Under torchrun the job's
+    targets are shared out over the ranks (dist.assign_tables: independent
+    tables, no data-path collective); each rank solves and writes its own
+    targets' tables on its GPU and rank 0 writes MANIFEST.JSON and
+    MODEL.JSON from every rank's records."""
+    from . import dist as pdist
+    rank, world, local = dist_ranks()
+    if device is None:
+        device = 0
+        if world > 1:
+            import torch
+            ngpu = torch.cuda.device_count() if torch.cuda.is_available() else 1
+            device = local if ngpu >= world else 0
     prep = Prepared(cfg)
     g, sp = prep.g, prep.sp
     cap = sp.cap
@@ -226,9 +260,12 @@ def run_solve(cfg, device: int = 0) -> dict:
     opts = _lib.default_opts(stop_rule=sp.stop_rule, storage=sp.storage,
                              warm_start=1 if sp.warm else 0, polish_sweeps=sp.polish_sweeps)
     ntargets = len(prep.states)
+    mine = pdist.assign_tables([prep.cells * sp.nctl] * ntargets, world)[rank]
     with _lib.Context(device) as ctx:
         ctx.load_problem(g.to_c(), prep.model.to_c(), sp.p, occ, sp.ctl, sp.storage)
         for ti, (name, s) in enumerate(zip(prep.names, prep.states)):
+            if ti not in mine:
+                continue
             seeds = seeds_for(g, s, sp, cfg)
             t0 = time.time()
             first = {"el": 0.0}
@@ -279,6 +316,10 @@ def run_solve(cfg, device: int = 0) -> dict:
                      bytes=info["bytes"], reached_frac=reached_frac, escape_frac=escape_frac,
                      escape_of_unreached_frac=esc_unr, elapsed_s=time.time() - t0)
 
+    if world > 1:
+        entries = pdist.gather_records(entries)
+    if rank != 0:
+        return {"targets": entries}
     r = sp.raw
     manifest = {
         "schema_version": 1,

@@ -4,7 +4,8 @@ CUDA library and a GPU).
     python tests/golden/make_card.py OUT_DIR
 
 Writes a seeded synthetic job (the 12x12x8x5x5x5 workload, seed 2, with a
-second target, the escape pass on, u16 tables) and runs
+second target, the escape pass on, 5 cm obstacle and 4 cm wall clearance,
+u16 tables) and runs
 `solve.py <config.json> solve` on it, so OUT_DIR gets TABLES/T##C####.BIN,
 MANIFEST.JSON and MODEL.JSON exactly as the wizard would receive them.  The
 committed copy is tests/golden/card_tiny/; tests/test_card_fixture.py checks
@@ -32,6 +33,14 @@ def main(out_dir: str) -> int:
         cfg = json.load(open(cfgp))
         cfg["escape"] = True
         cfg["escape_iterations"] = 30
+        # as the wizard writes a job: the table spans the field inset by the
+        # wall clearance (no pinned bounds).  4 cm, not 5: the card's table
+        # span is lo + step * (n - 1) in Float32, which for a 5 cm inset of
+        # this field lands 1.8e-5 cm past the inset, and the acceptance
+        # tool allows 1e-6 (the reference rounds the span identically)
+        del cfg["grid"]["bounds"]
+        cfg["clearance_cm"] = 5.0
+        cfg["wall_clearance_cm"] = 4.0
         tg = json.load(open(cfg["targets"]))
         first = tg["targets"][0]["state"]
         # a second target 60 cm away in x, clamped into the field

@@ -94,3 +94,44 @@ def test_cli_solve_writes_a_valid_card(tmp_path, escape):
     assert mj["control"]["saturation"]["knee"] > 0
     for name in ("A_s", "A_ss", "A_sgn", "A_absv"):
         assert all(all(v == 0 for v in row[:3]) for row in mj[name])
+
+
+def test_targets_shard_over_ranks(tmp_path):
+    """Under torchrun the job's targets are shared out over the ranks (two
+    ranks on one GPU here, gloo for the records: their solves never wait on
+    each other); the card equals the single-process card byte for byte."""
+    import shutil
+    import socket
+    sys.path.insert(0, PKG)
+    from peregrine_hjb.synth import write_job
+    cfgp = write_job(str(tmp_path / "job"), "tiny", seed=2)
+    cfg = json.load(open(cfgp))
+    tg = json.load(open(cfg["targets"]))
+    first = tg["targets"][0]["state"]
+    tg["targets"].append({"name": "second", "state": [first[0], first[1], 0.5, 0, 0, 0]})
+    tg["targets"].append({"name": "third", "state": [first[0], first[1], -1.0, 0, 0, 0]})
+    json.dump(tg, open(cfg["targets"], "w"))
+    json.dump(cfg, open(cfgp, "w"))
+    r = run_cli(cfgp)
+    assert r.returncode == 0, r.stderr[-2000:]
+    single = tmp_path / "single"
+    shutil.copytree(cfg["out_dir"], single)
+    shutil.rmtree(cfg["out_dir"])
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                        "--nproc-per-node", "2", "--master-addr", "127.0.0.1", "--master-port",
+                        str(port), os.path.join(PKG, "solve.py"), cfgp, "solve"],
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    m1 = json.load(open(single / "MANIFEST.JSON"))
+    m2 = json.load(open(os.path.join(cfg["out_dir"], "MANIFEST.JSON")))
+    assert [t["sha256"] for t in m1["targets"]] == [t["sha256"] for t in m2["targets"]]
+    assert len(m2["targets"]) == 3
+    for t in m1["targets"]:
+        for c in range(t["n_chunks"]):
+            a = open(single / (t["file_pattern"] % c), "rb").read()
+            b = open(os.path.join(cfg["out_dir"], t["file_pattern"] % c), "rb").read()
+            assert a == b
