@@ -174,6 +174,46 @@ def test_one_sweep_small_slab_bit_exact(og):
     assert np.array_equal(gam[lo:hi], am[lo:hi])
 
 
+TIE = 1e-5  # s: best two lookaheads closer than this are a tie (argmin not compared)
+
+
+def test_one_sweep_medium_slab_register_sweep(og):
+    """The benchmarked sweep (k_stencil_r) on the 48x48x32x15x15x15 workload
+    (125 controls) against the oracle on 12 y rows of the target's x row:
+    one sweep from a structured table within FMA_SWEEP_TOL, the same cells
+    left at the cap (every admissibility decision alike), and the argmin of
+    every cell whose best two lookaheads differ by more than TIE (checked on
+    a sample through the oracle's per-control lookaheads)."""
+    pr = Problem("medium", seed=0)
+    g, m, p = oracle_structs(og, pr)
+    n = pr.grid.n
+    per_x = pr.ncells // n[0]
+    per_y = per_x // n[1]
+    tx, ty = int(pr.seeds[0]) // per_x, (int(pr.seeds[0]) % per_x) // per_y
+    y0 = min(max(ty - 6, 0), n[1] - 12)
+    lo, hi = tx * per_x + y0 * per_y, tx * per_x + (y0 + 12) * per_y
+    with gpu_ctx(pr) as ctx:
+        ctx.set_value(init_value(pr))
+        for it in range(20):
+            ctx.sweep(phase=it, kernel=_lib.KERNEL_STENCIL)
+        Vk = ctx.get_value()
+        _, _, gam = ctx.sweep(phase=20, kernel=_lib.KERNEL_STENCIL, argmin=True)
+        got = ctx.get_value()[lo:hi]
+    want, _, _ = og.sweep_jacobi_slab(Vk, pr.occ, g, m, pr.ctl, p, lo, hi, phase=20)
+    cap = np.float32(pr.params.cap)
+    assert np.count_nonzero(want < cap) > 0.05 * (hi - lo)  # the slab carries structure
+    assert np.array_equal(got == cap, want == cap)
+    assert np.max(np.abs(got.astype(np.float64) - want)) <= FMA_SWEEP_TOL
+    rng = np.random.default_rng(1)
+    cells = lo + np.flatnonzero(want < cap)
+    cells = np.sort(rng.choice(cells, size=min(20000, cells.size), replace=False))
+    la = og.cell_lookaheads(Vk, pr.occ, g, m, pr.ctl, p, cells).astype(np.float64)
+    two = np.sort(la, axis=1)[:, :2]
+    clear = (two[:, 1] - two[:, 0] > TIE) & (two[:, 0] < cap)
+    assert clear.sum() > 0.5 * cells.size
+    assert np.array_equal(gam[cells[clear]], np.argmin(la[clear], axis=1))
+
+
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tiny_fixed_point.npz")
 
 
