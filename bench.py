@@ -59,32 +59,61 @@ def peaks():
     return 6650.0, "of fallback (no MEASURED_PEAKS.json: an earlier copy measurement on this pool)"
 
 
+def blend_tiling(n1: int, n2: int) -> tuple:
+    """(tile rows, row groups) of the register-resident sweep, the library's
+    rule: a block's first groups * n2 threads own one column of four window
+    rows each (4 groups >= rows + 3, groups * n2 <= 512, blocks of a multiple
+    of 32 threads, at least 64); per candidate -- the most rows the groups
+    allow, balanced over the plane -- the work per tile cell (50 per group
+    blended, 55 per group of cells shifted, 10 per idle thread) and the warps
+    per SM (512 threads); the cheapest with at least 12 warps per SM wins."""
+    def cand(tx):
+        groups = (tx + 6) // 4
+        block = 32 * ((groups * n2 + 31) // 32)
+        if block > 512:
+            return None
+        live = (tx + 3) // 4
+        block = max(64, block)
+        cost = (50.0 * groups * n2 + 55.0 * live * n2 + 10.0 * (block - groups * n2)) / (tx * n2)
+        return (tx, groups, cost, (512 // block) * (block // 32))
+    pick = None
+    groups = 1
+    while groups * n2 <= 512:
+        txmax = min(n1, 4 * groups - 3)
+        if txmax >= 1:
+            nt = -(-n1 // txmax)
+            c = cand(-(-n1 // nt))
+            if c and (pick is None or ((c[3] >= 12) != (pick[3] >= 12) and c[3] >= 12)
+                      or ((c[3] >= 12) == (pick[3] >= 12) and c[2] < pick[2])):
+                pick = c
+        groups += 1
+    if pick is None:
+        raise ValueError(f"no register-resident tiling for {n2} columns")
+    return pick[0], pick[1]
+
+
 def blend_tile_rows(n1: int, n2: int) -> int:
-    """Rows per block of the register-resident sweep (the library's tiling:
-    whole rows whose window of rows + 3 fits 1024 cells when the 3 extra rows
-    cost at most a quarter, else 2048 cells, balanced over the plane)."""
-    t1 = min(n1, 1024 // n2 - 3)
-    t2 = min(n1, 2048 // n2 - 3)
-    tx = t1 if t1 >= 1 and (t1 == n1 or 4 * (t1 + 3) <= 5 * t1) else t2
-    nt = -(-n1 // tx)
-    return -(-n1 // nt)
+    return blend_tiling(n1, n2)[0]
 
 
 def onchip_rooflines(pr, rate_per_gpu: float, elem: int, peaks_onchip) -> dict:
     """The sweep's on-chip ceilings.  Per cell-control the register-resident
-    kernel blends 16 corner values held in registers into (TX+3)/TX window
-    values, writes them to shared memory as FP32 and reads back 4 of them,
-    the row and column successor entries (8 B each) and the mask word (a
-    warp-wide broadcast); it spends 16 (TX+3)/TX + 3 FMAs plus three subtracts
-    and an add.  (The corner planes are read from L2 once per group of
-    controls, not per control.)"""
+    kernel blends 16 corner values held in registers into 4 G / TX window
+    values (G row groups of four rows for TX tile rows), writes them to
+    shared memory as FP32, and for its four cells of one column reads five
+    window rows of two values (2.5 rows per cell when the successor rows are
+    consecutive), a row entry of 32 B per four cells, a column entry of 8 B
+    per four cells and a warp's mask words (a broadcast); it spends
+    16 (4 G / TX) + 3 FMAs plus three subtracts and an add.  (The corner
+    planes are read from L2 once per group of controls, not per control.)"""
     n1, n2 = int(pr.grid.n[0]), int(pr.grid.n[1])
-    tx = blend_tile_rows(n1, n2)
-    win = (tx + 3) / tx
+    tx, groups = blend_tiling(n1, n2)
+    win = 4.0 * groups / tx
     del elem  # the storage type only changes the once-per-group loads
-    bytes_cc = 4 * win + 16 + 8 + 8 + 4 / 32
+    bytes_cc = 4 * win + 10 + 8 + 2 + 4 / 32
     flops_cc = 2 * (16 * win + 3) + 4
-    out = {"tile_rows": tx, "bytes_per_update": bytes_cc, "flops_per_update": flops_cc}
+    out = {"tile_rows": tx, "row_groups": groups, "bytes_per_update": bytes_cc,
+           "flops_per_update": flops_cc}
     if peaks_onchip:
         g = rate_per_gpu * bytes_cc / 1e9
         f = rate_per_gpu * flops_cc / 1e12
@@ -427,9 +456,10 @@ def run_accuracy(args, local_rank):
     followed by FP32 polish sweeps -- is solved to a ladder of max-norm stop
     tolerances, and the device time of the cheapest run within 2 ms of the
     reference is its time-to-converge.  Errors against the FP64 table
-    (max-norm 1e-9 s) are reported beside them: FP64 also decides the probe
-    and range tests in double, so near obstacles a few cells can differ from
-    every FP32 answer by more than the convergence error."""
+    (max-norm 1e-9 s) are reported beside them: FP64 storage runs the
+    precision oracle (the FP32 solver's admissibility and successor
+    decisions, FP64 interpolation, min and residual), so that difference is
+    the FP32 arithmetic's, not a different model's."""
     import numpy as np
     import torch
     from peregrine_hjb import _lib
@@ -488,6 +518,101 @@ def run_accuracy(args, local_rank):
     return 0
 
 
+def _max_rms_over(V, ref, cap, device, chunk=1 << 27):
+    """max and RMS of |V - ref| over the reached cells (0 < ref < cap - 1 ms)
+    of two host tables, in chunks on the device."""
+    import torch
+    mx, ss, n = 0.0, 0.0, 0
+    for i in range(0, ref.size, chunk):
+        r = torch.from_numpy(ref[i:i + chunk]).to(device)
+        v = torch.from_numpy(V[i:i + chunk]).to(device)
+        m = (r > 0) & (r < cap - 1e-3)
+        e = (v.double() - r.double()).abs()[m]
+        if e.numel():
+            mx = max(mx, float(e.max()))
+            ss += float((e * e).sum())
+            n += int(e.numel())
+    return mx, math.sqrt(ss / max(n, 1)), n
+
+
+def run_converge(args, local_rank):
+    """Time-to-converge of plain FP32 value iteration on one table from one
+    trajectory, for grids too large to solve once per stop tolerance: the
+    benchmarked sweep runs from the initial table (cap everywhere, zero at
+    the targets) until no cell changes by more than 1e-9 s (the table's own
+    fixed point, the reference answer); at the first sweep whose max-norm
+    change is within each tolerance of --tols the table is copied to host
+    memory, and afterwards each copy is compared with the fixed point over
+    the reached cells.  The time of a stop tolerance is the sweeps' device
+    time up to that sweep; the time-to-converge is the least time whose table
+    lies within 2 ms of the fixed point.  With --storages fp16, an FP16
+    solve followed by FP32 polish sweeps (the library's 16-bit pattern) is
+    then made at each tolerance and compared with the same fixed point."""
+    import numpy as np
+    import torch
+    from peregrine_hjb import _lib
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    pr = problem_for_rank(0)
+    cap = float(pr.params.cap)
+    ladder = sorted((float(t) for t in args.tols.split(",")), reverse=True)
+    snaps = []
+    ctx = _lib.Context(local_rank)
+    try:
+        ctx.load_problem(pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.ctl, "fp32")
+        opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL)
+        ctx.solve(pr.seeds, 0, 0.0, opts)  # the initial table, no sweep
+        dev_s, it, k, dm, trace = 0.0, 0, 0, float("inf"), []
+        while it < args.max_sweeps and dm > 1e-9:
+            t0 = time.perf_counter()
+            d, dm, _ = ctx.sweep(phase=it, kernel=_lib.KERNEL_STENCIL)
+            dev_s += time.perf_counter() - t0
+            it += 1
+            if it % 25 == 0:
+                trace.append([it, dm])
+            while k < len(ladder) and dm <= ladder[k]:
+                snaps.append({"tol": ladder[k], "sweeps": it, "sweep_s": dev_s, "V": ctx.get_value()})
+                k += 1
+        ref = ctx.get_value()
+        ref_sweeps, ref_s = it, dev_s
+    finally:
+        ctx.close()
+    rows = []
+    for s in snaps:
+        mx, rms, n = _max_rms_over(s.pop("V"), ref, cap, dev)
+        s.update(max_err=mx, rms_err=rms)
+        rows.append(s)
+    ok = [r["sweep_s"] for r in rows if r["max_err"] <= 2e-3]
+    line = {"report": "time_to_converge_trajectory", "workload": WORKLOAD, "cells": pr.ncells,
+            "controls": pr.nctl, "target_max_err_s": 2e-3, "storage": "fp32",
+            "kernel": "k_stencil_r (the benchmarked sweep)",
+            "timing": "host clock around the synchronous per-sweep calls (the sweep on the "
+                      "device plus one residual read-back per sweep)",
+            "reference": {"stop": "max-norm <= 1e-9 s (its own fixed point)", "sweeps": ref_sweeps,
+                          "sweep_s": ref_s},
+            "error_over": "reached cells (0 < V < cap - 1 ms)", "fp32": rows,
+            "maxnorm_every_25_sweeps": trace,
+            "time_to_converge_s": {"fp32": min(ok) if ok else None}}
+    if "fp16" in args.storages.split(","):
+        line["fp16"] = []
+        for s in rows:
+            opts = _lib.default_opts(stop_rule=_lib.STOP_MAXNORM, kernel=_lib.KERNEL_STENCIL,
+                                     storage="fp16", polish_sweeps=args.max_sweeps)
+            V, res = _lib.solve_value(pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.seeds,
+                                      pr.ctl, args.max_sweeps, s["tol"], opts, device=local_rank)
+            mx, rms, _ = _max_rms_over(V, ref, cap, dev)
+            line["fp16"].append({"tol": s["tol"], "sweeps": res.iterations - res.polish_iterations,
+                                 "polish_sweeps": res.polish_iterations,
+                                 "kernel_s": res.kernel_ms / 1000.0, "max_err": mx, "rms_err": rms})
+            if mx <= 2e-3:
+                break
+        ok16 = [r["kernel_s"] for r in line["fp16"] if r["max_err"] <= 2e-3]
+        line["time_to_converge_s"]["fp16"] = min(ok16) if ok16 else None
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -503,6 +628,9 @@ def main():
     ap.add_argument("--accuracy", action="store_true",
                     help="time-to-converge and FP32/FP64/FP16/BF16 error report instead of "
                          "the throughput line")
+    ap.add_argument("--converge", action="store_true",
+                    help="time-to-converge of one FP32 trajectory with snapshots at --tols "
+                         "(for grids too large for --accuracy)")
     ap.add_argument("--storages", default="fp32,fp16,bf16,q16,q16-nopolish",
                     help="storages of the accuracy report; -nopolish: no FP32 polish")
     ap.add_argument("--no-fp64", action="store_true",
@@ -521,6 +649,8 @@ def main():
         return run_reference(args, rank, world)
     if args.accuracy:
         return run_accuracy(args, local_rank)
+    if args.converge:
+        return run_converge(args, local_rank)
     if world > 1:
         import datetime
         import torch

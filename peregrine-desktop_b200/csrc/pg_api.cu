@@ -189,41 +189,102 @@ int ensure_values(pg_ctx* ctx, int storage) {
     return PG_OK;
 }
 
-// Register-resident blend tiling: the window ((rows + 3) x Ny cells) takes
-// kRCellsPerThread cells per thread, at most 2048 cells.  rows = 0 picks: the
-// most rows whose window fits 1024 cells (two blocks per SM) when the three
-// extra window rows cost at most a quarter, else the most that fit 2048,
-// balanced over the plane; rows < 0 or a window that does not fit leaves the
-// tiling at 0 (not eligible).
+// Register-resident blend tiling.  A block of rblock threads (a multiple of
+// 32, at most 512) sweeps a tile of rtile_x rows: its first rgroups * Ny
+// threads own one column of four window rows each, so the window of
+// rtile_x + 3 rows needs 4 rgroups >= rtile_x + 3.  rows = 0 picks the tile
+// height: for each candidate (the most rows that rgroups groups allow,
+// balanced over the plane) the work per tile cell and control -- window
+// cells blended, plus cells shifted, plus idle threads -- and the resident
+// warps per SM (128 registers a thread); the cheapest with at least 12
+// warps per SM, else the cheapest.  rows < 0, or a tiling that cannot run,
+// leaves it at 0 (not eligible).  The controls a block stages at once
+// (rchunk) are all of them when they fit the shared memory that the blocks
+// the registers allow on an SM share (228 KB, less 1 KB reserved and 1 KB of
+// static shared memory per block), else as many as fit, with fewer blocks per SM only when fewer than 16
+// would fit.
+namespace {
+struct RTile {
+    int32_t tx = 0, groups = 0, block = 0;
+    double cost = 0.0;
+    int warps = 0;
+};
+RTile r_candidate(int32_t n1, int32_t n2, int32_t tx) {
+    RTile c;
+    if (tx < 1 || tx > n1) return c;
+    const int32_t groups = (tx + 3 + 3) / 4;
+    const int64_t block = 32 * (((int64_t)groups * n2 + 31) / 32);
+    if (block > 512) return c;
+    const int32_t live = (tx + 3) / 4;
+    c.tx = tx;
+    c.groups = groups;
+    c.block = (int32_t)std::max<int64_t>(64, block);
+    // instructions per thread and control: ~50 to blend four window cells,
+    // ~55 to shift four cells, ~10 for a thread that only waits
+    c.cost = (50.0 * groups * n2 + 55.0 * live * n2 + 10.0 * (c.block - (int64_t)groups * n2)) /
+             ((double)tx * n2);
+    c.warps = (512 / c.block) * (c.block / 32);
+    return c;
+}
+}  // namespace
+
 void r_tiling(pg::KParams& kp, int32_t rows) {
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
-    kp.rtile_x = kp.rtiles_x = kp.rblock = 0;
-    if (rows < 0 || n2 < 1 || n2 > 0xffff) return;
-    int32_t tx = rows;
-    if (tx <= 0) {
-        const int32_t t1 = std::min<int32_t>(n1, 1024 / n2 - 3);
-        const int32_t t2 = std::min<int32_t>(n1, 2048 / n2 - 3);
-        tx = (t1 >= 1 && (t1 == n1 || 4 * (t1 + 3) <= 5 * t1)) ? t1 : t2;
-        if (tx < 1) return;
-        const int32_t nt = (n1 + tx - 1) / tx;
-        tx = (n1 + nt - 1) / nt;
+    kp.rtile_x = kp.rtiles_x = kp.rblock = kp.rgroups = kp.rchunk = 0;
+    if (rows < 0 || n2 < 1 || n2 > 512 || kp.nctl < 1 || kp.nctl > (int)pg::kCtlMaskHost) return;
+    RTile pick;
+    if (rows > 0) {
+        pick = r_candidate(n1, n2, rows);
+    } else {
+        auto better = [](const RTile& a, const RTile& b) {  // a better than b
+            if (b.tx == 0) return a.tx != 0;
+            if (a.tx == 0) return false;
+            const bool aw = a.warps >= 12, bw = b.warps >= 12;
+            if (aw != bw) return aw;
+            return a.cost < b.cost;
+        };
+        for (int32_t groups = 1; groups * n2 <= 512; ++groups) {
+            const int32_t txmax = std::min<int32_t>(n1, 4 * groups - 3);
+            if (txmax < 1) continue;
+            const int32_t nt = (n1 + txmax - 1) / txmax;
+            const RTile c = r_candidate(n1, n2, (n1 + nt - 1) / nt);
+            if (better(c, pick)) pick = c;
+        }
     }
-    const int64_t win = (int64_t)(tx + 3) * n2;
-    if (tx < 1 || tx > n1 || win > pg::kRMaxWindowHost) return;
-    kp.rtile_x = tx;
-    kp.rtiles_x = (n1 + tx - 1) / tx;
-    const int64_t kc = pg::kRCellsPerThread;
-    kp.rblock = (int32_t)std::max<int64_t>(64, 32 * (((win + kc - 1) / kc + 31) / 32));
+    if (pick.tx == 0) return;
+    kp.rtile_x = pick.tx;
+    kp.rtiles_x = (n1 + pick.tx - 1) / pick.tx;
+    kp.rgroups = pick.groups;
+    kp.rblock = pick.block;
+    // controls staged at once: all of them if the blocks that the registers
+    // allow on an SM (up to two) fit in its shared memory, else all that fit
+    // one block per SM, else as many as fit
+    const size_t per = pg::stencil_r_ctl_smem_bytes(kp, pick.tx);
+    kp.rchunk = 1;
+    const size_t fixed = pg::stencil_r_smem_bytes(kp) - per + 16;
+    const int bps = std::min(4, 512 / pick.block);
+    int32_t chunk = 0;
+    for (int b = bps; b >= 1; --b) {
+        // 228 KB per SM; per block 1 KB reserved and up to 1 KB of static
+        // shared memory
+        const size_t lim = std::min<size_t>((size_t)pg::kRSmemMax, ((size_t)228 / b - 2) * 1024);
+        const int64_t c = lim > fixed ? (int64_t)((lim - fixed) / per) : 0;
+        chunk = (int32_t)std::min<int64_t>(c, kp.nctl);
+        // as many blocks per SM as the registers allow, while a block still
+        // stages a useful number of controls at once
+        if (chunk >= std::min(kp.nctl, 16)) break;
+    }
+    if (chunk < 1) {
+        kp.rtile_x = kp.rtiles_x = kp.rblock = kp.rgroups = kp.rchunk = 0;
+        return;
+    }
+    kp.rchunk = chunk;
 }
 
-// The register-resident blend keeps every control's successor corners in
-// shared memory; it runs where that leaves room for two blocks per SM (228 KB
-// of shared memory per SM less 1 KB reserved per block; or,
-// with more than 256 threads, the block has the SM to itself anyway) and the
-// re-reading blend runs elsewhere.
+// Whether the register-resident blend's tiling is set and runs.
 bool r_smem_fits(const pg::KParams& kp) {
-    return kp.rtile_x > 0 &&
-           pg::stencil_r_smem_bytes(kp) <= (size_t)(kp.rblock > 256 ? 200 : 110) * 1024;
+    return kp.rtile_x > 0 && pg::stencil_r_shape_ok(kp) &&
+           pg::stencil_r_smem_bytes(kp) <= (size_t)pg::kRSmemMax;
 }
 
 // Planes of row-order mask words that fit a staging buffer of `bytes`.
@@ -710,8 +771,7 @@ int load_impl(pg_ctx* ctx, const pg_grid6* g_in, const pg_model* m, const pg_par
     if (ctx->stencil_ok && !slab) {
         const size_t mb = pg::stencil_mask_bytes(kp), rb = pg::stencil_recs_bytes(kp);
         const size_t gb = (size_t)kp.nplanes * kp.nctl * sizeof(uint16_t);
-        const bool r_able = storage != PG_STORE_F64 && kp.rtile_x > 0 && kp.nctl <= 0x7fff &&
-                            r_smem_fits(kp);
+        const bool r_able = storage != PG_STORE_F64 && r_smem_fits(kp);
         const size_t tb = r_able ? pg::stencil_tmask_bytes(kp) : 0;
         const size_t G = (size_t)1 << 30;
         size_t fr = 0, tot = 0;
@@ -1225,10 +1285,10 @@ int pg_set_tile_rows(pg_ctx* ctx, int32_t rows) {
     pg::KParams& kp = ctx->kp;
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
     const bool b_fits = (int64_t)rows * n2 <= pg::kBMaxTileCells;
-    const bool r_fits = (int64_t)(rows + 3) * n2 <= pg::kRMaxWindowHost;
+    const bool r_fits = (int64_t)((rows + 6) / 4) * n2 <= pg::kRMaxWindowHost / 4;
     if (rows < 1 || rows > n1 || !(b_fits || r_fits))
         return fail(PG_EINVAL, "tile rows must be in [1, Nx] with rows * Ny <= 1024 or "
-                               "(rows + 3) * Ny <= 2048");
+                               "ceil((rows + 3) / 4) * Ny <= 512");
     const int32_t nt = (n1 + rows - 1) / rows;
     const int64_t need = kp.nplanes * nt;
     if (need > ctx->nparts) {

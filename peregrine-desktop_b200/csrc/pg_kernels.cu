@@ -1055,7 +1055,7 @@ static cudaError_t r_batch_attr() {
     const uint64_t attr_bit = device_bit();
     if (attr_set.load() & attr_bit) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_stencil_r_batch<S, kRCellsPerThread>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kRSmemMax);
     if (e == cudaSuccess) attr_set.fetch_or(attr_bit);
     return e;
 }
@@ -1085,7 +1085,7 @@ cudaError_t launch_stencil_r_batch(int storage, const BatchTable* tabs, int ntab
                                    double* part_sum, double* part_max, size_t smem, int grid,
                                    cudaStream_t st) {
     if (threads <= 0 || threads > RShape<kRCellsPerThread>::kMaxThreads || threads % 32 != 0 ||
-        grid <= 0 || smem > 200 * 1024)
+        grid <= 0 || smem > (size_t)kRSmemMax)
         return cudaErrorInvalidValue;
 #define PG_RB(S)                                                                                 \
     {                                                                                            \
@@ -1128,22 +1128,19 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
                                const uint32_t* recs, const uint32_t* tmask, const KParams& kp,
                                const uint16_t* gord, const SweepBufs& sb, int16_t* argmin,
                                cudaStream_t st, int64_t* launches) {
-    if (kp.rtile_x <= 0 || kp.rblock <= 0 || kp.rblock > RShape<KR>::kMaxThreads ||
-        kp.rblock % 32 != 0 || (KR * (kp.rblock / 32)) % 4 != 0 || kp.nsub > kStencilMaxSub ||
-        kp.g.n[1] > 0xffff || (int64_t)(kp.rtile_x + 3) * kp.g.n[1] > (int64_t)kp.rblock * KR)
-        return cudaErrorInvalidValue;
+    if (!stencil_r_shape_ok(kp)) return cudaErrorInvalidValue;
     KParams kr = kp;
     kr.tile_x = kp.rtile_x;
     kr.tiles_x = kp.rtiles_x;
     const int64_t blocks = kp.nplanes * kp.rtiles_x;
     if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-    const size_t smem = stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, KR, kp.nsub);
-    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    const size_t smem = stencil_r_smem_bytes(kp);
+    if (smem > (size_t)kRSmemMax) return cudaErrorInvalidValue;
     static std::atomic<uint64_t> attr_set{0};
     const uint64_t attr_bit = device_bit();
     if (!(attr_set.load() & attr_bit)) {
         cudaError_t e = cudaFuncSetAttribute(k_stencil_r<S, ARGMIN, KR>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kRSmemMax);
         if (e != cudaSuccess) return e;
         attr_set.fetch_or(attr_bit);
     }
@@ -1235,7 +1232,20 @@ size_t stencil_tmask_bytes(const KParams& kp) {
 }
 
 size_t stencil_r_smem_bytes(const KParams& kp) {
-    return stencil_r_smem(kp.nctl, kp.rtile_x, kp.g.n[1], kp.rblock, kRCellsPerThread, kp.nsub);
+    return stencil_r_smem(kp.nctl, kp.rchunk, kp.rtile_x, kp.g.n[1], kp.rgroups, kp.nsub);
+}
+
+bool stencil_r_shape_ok(const KParams& kp) {
+    const int32_t n2 = kp.g.n[1];
+    return kp.rtile_x > 0 && kp.rtiles_x > 0 && kp.rblock > 0 &&
+           kp.rblock <= RShape<kRCellsPerThread>::kMaxThreads && kp.rblock % 32 == 0 &&
+           kp.rgroups > 0 && (int64_t)kp.rgroups * n2 <= kp.rblock &&
+           kp.rtile_x + 3 <= 4 * kp.rgroups && kp.rchunk > 0 && kp.rchunk <= kp.nctl &&
+           kp.nctl <= (int)kCtlMask && kp.nsub <= kStencilMaxSub && n2 >= 1 && n2 <= 0xffff;
+}
+
+size_t stencil_r_ctl_smem_bytes(const KParams& kp, int32_t tile_x) {
+    return stencil_r_ctl_bytes(tile_x, kp.g.n[1], kp.nsub);
 }
 
 size_t stencil_b_smem_bytes(const KParams& kp) {

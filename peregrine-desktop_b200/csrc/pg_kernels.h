@@ -65,6 +65,11 @@ cudaError_t launch_stencil_tmask(const uint32_t* mask, const KParams& kp, int64_
                                  int64_t nplanes, uint32_t* tmask, cudaStream_t st,
                                  int64_t* launches);
 size_t stencil_r_smem_bytes(const KParams& kp);
+// whether kp's register-resident tiling (rtile_x, rgroups, rblock, rchunk)
+// is one k_stencil_r can run
+bool stencil_r_shape_ok(const KParams& kp);
+// shared memory one staged control takes in a k_stencil_r block of tile_x rows
+size_t stencil_r_ctl_smem_bytes(const KParams& kp, int32_t tile_x);
 size_t stencil_tmask_bytes(const KParams& kp);
 cudaError_t launch_stencil_b_batch(int storage, const BatchTable* tabs, int ntab, int64_t first,
                                    int64_t count, int threads, int parity, const int32_t* done,

@@ -12,22 +12,27 @@
 //
 //   k_stencil_group (once per solve) sorts each plane's controls by their
 //   (corner planes, x offset) and flags the first control of each group;
-//   controls that no cell of the plane admits go last;
+//   controls that no cell of the plane admits go last, flagged;
 //
 //   k_stencil_tmask (once per tiling) regroups the admissibility mask per
-//   (plane, tile, control) in tile order;
+//   (plane, tile, control) in the order the sweep's threads read it;
 //
-//   k_stencil_r copies a block's per-control data (weights, tau, offsets,
-//   substep increments, mask words) into shared memory with asynchronous
-//   copies, computes from the staged increments every control's per-row and
-//   per-column successor corners and fractions (which k_stencil_b
-//   recomputes per control; here many independent chains per thread, once
-//   per block), loads at the first control of each group the 16 corner
-//   values of each of its window cells into registers (KR cells per
-//   thread), and for every control of the group blends them with the
-//   control's 16 weights -- 16 FMAs per window cell from registers, nothing
-//   re-read -- into the shared window, then shifts exactly as k_stencil_b
-//   does.
+//   k_stencil_r: block = (plane, tile of TX rows).  Thread (g, j) of the
+//   first G * Ny owns column j of the four window rows 4g .. 4g+3 and of the
+//   tile cells in those rows.  The block stages its controls' weights, tau,
+//   offsets, substep increments and mask words into shared memory with
+//   asynchronous copies (a chunk of controls at a time when they do not all
+//   fit), computes from the increments every control's per-row and
+//   per-column successor corners and fractions, and walks the controls in
+//   group order.  At the first control of a group each thread loads the 16
+//   corner values of its four window cells into registers; for every control
+//   it blends them with the control's 16 weights (16 FMAs per window cell,
+//   two cells per packed fma.rn.f32x2, nothing re-read) into the shared
+//   window; then it shifts: its four cells lie in consecutive rows of one
+//   column, and the successor rows of consecutive rows are nearly always
+//   consecutive too, so the four bilinear steps read five window rows (ten
+//   values) instead of eight, the column entry once, the row entries and
+//   the mask words as one vector each.
 //
 // The arithmetic is k_stencil_b's, operation for operation: the same FMA
 // chain over the corners in record order, the same per-row / per-column
@@ -50,23 +55,20 @@ __device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
     return d;
 }
-// a - b per lane, IEEE round to nearest (sub.rn.f32x2)
-__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
 
 // Controls of a plane in group order: entry = control | kGroupFirst on the
-// first control of a group.
+// first control of a group | kCtlInadmissible when no cell of the plane
+// admits it (those come last).
 constexpr uint16_t kGroupFirst = 0x8000u;
+constexpr uint16_t kCtlInadmissible = 0x4000u;
+constexpr uint16_t kCtlMask = 0x3fffu;
+static_assert(kCtlMask == kCtlMaskHost, "the host's control limit is the group order's");
 static_assert(kRMaxWindowHost == 4 * 512, "window cells per block: 4 per thread, 512 threads");
 
 // Threads per block at most and the minimum resident blocks for KR window
-// cells per thread: 16 KR corner registers per thread, so KR = 2 keeps 64
-// registers and up to 1024 threads; KR = 4, 128 registers and 512 threads.
+// cells per thread: 16 KR corner registers per thread, so KR = 4 keeps 64 of
+// them and allows up to 512 threads (128 registers each).
 template <int KR> struct RShape;
-template <> struct RShape<2> { static constexpr int kMaxThreads = 1024, kMinBlocks = 1; };
 template <> struct RShape<4> { static constexpr int kMaxThreads = 512, kMinBlocks = 1; };
 
 __host__ __device__ inline size_t stencil_group_smem(int nctl) {
@@ -115,7 +117,9 @@ __global__ void __launch_bounds__(128)
             const int32_t *a = key + u * 17, *b = key + srt[r - 1] * 17;
             for (int f = 0; f < 17 && !first; ++f) first = a[f] != b[f];
         }
-        gord[(size_t)pl * nctl + r] = (uint16_t)u | (first ? kGroupFirst : 0u);
+        const bool ok = key[u * 17] != 0x7fffffff;
+        gord[(size_t)pl * nctl + r] =
+            (uint16_t)((uint32_t)u | (first ? kGroupFirst : 0u) | (ok ? 0u : kCtlInadmissible));
     }
 }
 
@@ -140,17 +144,22 @@ __device__ __forceinline__ void succ_li_t(const pg_grid6& g, const float* inc, i
     *li = (int32_t)fminf(fmaxf(fl, -2.0f), (float)(row ? n1 + 2 : n2 + 2));
 }
 
-// Words of one tile's admissibility bits in tile order (bit e of the tile =
-// cell e = a * n2 + j of its rows), rounded up to whole 16-byte pieces: the
-// stride of one (plane, tile, control)'s words in the tile-order mask.
+// Row groups of a tile of tile_x rows that hold cells (four rows each), the
+// warps whose threads own those cells, and the mask words per (plane, tile,
+// control): four per such warp (one per row of the group, bit = lane).
+__host__ __device__ inline int32_t stencil_r_live_groups(int32_t tile_x) { return (tile_x + 3) >> 2; }
+__host__ __device__ inline int32_t stencil_r_live_warps(int32_t tile_x, int32_t n2) {
+    return (stencil_r_live_groups(tile_x) * n2 + 31) >> 5;
+}
 __host__ __device__ inline int32_t tile_mask_stride(int32_t tile_x, int32_t n2) {
-    return ((tile_x * n2 + 31) / 32 + 3) & ~3;
+    return 4 * stencil_r_live_warps(tile_x, n2);
 }
 
-// The admissibility mask regrouped per (plane, tile, control) in tile order,
-// from the per-row layout of k_stencil_prep, for the planes [plane0,
-// plane0 + nplanes) whose row-order words `mask` holds (plane plane0 first);
-// tstride words per control, zero past the tile's cells.
+// The admissibility mask regrouped per (plane, tile, control) in thread
+// order, from the per-row layout of k_stencil_prep, for the planes [plane0,
+// plane0 + nplanes) whose row-order words `mask` holds (plane plane0 first):
+// word 4 w + q holds, in bit l, the cell of thread t = 32 w + l in row
+// 4 (t / Ny) + q of the tile, column t % Ny (0 past the tile's rows).
 __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, int32_t tile_x,
                                 int32_t tiles_x, int32_t tstride, int64_t plane0, int64_t nplanes,
                                 uint32_t* __restrict__ tmask) {
@@ -161,100 +170,127 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         int64_t r = i / tstride;
-        const int32_t w = (int32_t)(i - r * tstride);
+        const int32_t wq = (int32_t)(i - r * tstride);
+        const int32_t w = wq >> 2, q = wq & 3;
         const int32_t u = (int32_t)(r % nctl);
         r /= nctl;
         const int32_t xt = (int32_t)(r % tiles_x);
         const int64_t pl = r / tiles_x;
         const int32_t x0 = xt * tile_x;
-        const int32_t ncell = min(tile_x, n1 - x0) * n2;
+        const int32_t nr = min(tile_x, n1 - x0);
         const uint32_t* mrow = mask + ((size_t)pl * nctl + u) * n1 * W;
         uint32_t word = 0;
-        // bits 32w .. 32w+31 of the tile: runs of consecutive columns of one
-        // row, each taken from at most two of the row's words
-        const int32_t e0 = 32 * w, e1 = min(e0 + 32, ncell);
-        int32_t e = e0;
-        int32_t a = e / n2, j = e - a * n2;
-        while (e < e1) {
-            const int32_t len = min(e1 - e, n2 - j);  // 1..32
-            const uint32_t* rw = mrow + (x0 + a) * W;
-            const int32_t wi = j >> 5;
-            const uint32_t lo = __ldg(rw + wi);
-            const uint32_t hi = (wi + 1 < W) ? __ldg(rw + wi + 1) : 0u;
-            const uint32_t bits = __funnelshift_r(lo, hi, (uint32_t)(j & 31));
-            const uint32_t keep = len >= 32 ? 0xffffffffu : ((1u << len) - 1u);
-            word |= (bits & keep) << (e - e0);
-            e += len;
-            j = 0;
-            ++a;
+        // the warp's 32 threads: runs of consecutive columns of one row,
+        // each taken from at most two of the row's words
+        const int32_t t0 = 32 * w, t1 = t0 + 32;
+        int32_t t = t0;
+        while (t < t1) {
+            const int32_t g = t / n2, j = t - g * n2;
+            const int32_t len = min(t1 - t, n2 - j);  // 1..32
+            const int32_t a = 4 * g + q;
+            if (a < nr) {
+                const uint32_t* rw = mrow + (x0 + a) * W;
+                const int32_t wi = j >> 5;
+                const uint32_t lo = __ldg(rw + wi);
+                const uint32_t hi = (wi + 1 < W) ? __ldg(rw + wi + 1) : 0u;
+                const uint32_t bits = __funnelshift_r(lo, hi, (uint32_t)(j & 31));
+                const uint32_t keep = len >= 32 ? 0xffffffffu : ((1u << len) - 1u);
+                word |= (bits & keep) << (t - t0);
+            }
+            t += len;
         }
         out[i] = word;
     }
 }
 
-// Shared memory of one k_stencil_r block of `threads` threads (a multiple of
-// 32) with KR cells per thread: the plane's group order; per control a
-// parameter area of kRWt + 2 NI words -- staged as its record's weights,
-// tau, offsets, admissibility and substeps (24 words) and its substep
-// position increments (x, then y, NI words each), and once the successor
-// entries are made, rewritten as the 16 weights each duplicated into an
-// FP32 pair (32 words) and the 8 parameter words; its mask words (one per
-// warp and cell slot, a warp's KR words together, zero past the tile's);
-// its successor entries (the tile's rows, then every column); and two
-// padded window buffers with room for every thread's KR window slots (slots
-// past the window land in scratch rows).
+// Shared memory of one k_stencil_r block: the plane's group order (all
+// controls); per staged control a parameter area of kRWt + 2 NI words --
+// staged as its record's weights, tau, offsets, admissibility and substeps
+// (24 words) and its substep position increments (x, then y, NI words
+// each), and once the successor entries are made, rewritten as the 16
+// weights each duplicated into an FP32 pair (32 words) and 8 parameter
+// words --, its mask words, its row entries (per live row group: the four
+// rows' window offsets in bytes, then their x fractions) and its column
+// entries (per column: the lower column's byte offset and the y fraction);
+// then two window buffers of 4 G rows of stencil_r_row_stride(Ny) floats.
+// Window row stride in floats: at least Ny + 1 (one padding column), and,
+// when Ny is a multiple of 4, such that rows four apart differ by Ny mod 32
+// banks -- a warp whose lanes straddle two row groups (the end of row 4g,
+// the start of row 4g + 4) then touches each bank once.
+__host__ __device__ inline int32_t stencil_r_row_stride(int32_t n2) {
+    int32_t sb = n2 + 1;
+    if ((n2 & 3) == 0)
+        while (((4 * sb - n2) & 31) != 0) ++sb;
+    return sb;
+}
 constexpr int kRWt = 24;  // as staged: w[16], tau, tx, ty, -, ox, oy, ok, nsub
-// as rewritten: (w, w) pairs in words 0-31, then tau, tx, ty, -, ox, oy, ok, nsub
-constexpr int kRTau = 32, kROx = 36, kROk = 38;
+// as rewritten: (w, w) pairs in words 0-31, then tau, tx, ty, next, ox, oy,
+// ok, nsub; next = 1 when the following control starts a new group
+constexpr int kRTau = 32, kRNext = 35;
 // x and y increments per control: at least 8 each, so that the parameter
 // area holds the rewritten 40 words
 __host__ __device__ inline int32_t stencil_r_ninc(int nsub) {
     const int32_t n = (nsub + 3) & ~3;
     return n > 8 ? n : 8;
 }
-__host__ __device__ inline int32_t stencil_r_window_rows(int tile_x, int n2, int threads, int kr) {
-    const int32_t slots = (kr * threads + n2 - 1) / n2;
-    return slots > tile_x + 3 ? slots : tile_x + 3;
+__host__ __device__ inline size_t stencil_r_ctl_bytes(int tile_x, int n2, int nsub) {
+    return (size_t)(kRWt + 2 * stencil_r_ninc(nsub)) * 4 + (size_t)tile_mask_stride(tile_x, n2) * 4 +
+           (size_t)stencil_r_live_groups(tile_x) * 32 + (size_t)n2 * 8;
 }
-__host__ __device__ inline size_t stencil_r_smem(int nctl, int tile_x, int n2, int threads, int kr,
+__host__ __device__ inline size_t stencil_r_smem(int nctl, int chunk, int tile_x, int n2, int groups,
                                                  int nsub) {
-    return (size_t)((nctl + 7) & ~7) * 2 + (size_t)nctl * kRWt * 4 +
-           (size_t)nctl * 2 * stencil_r_ninc(nsub) * 4 + (size_t)nctl * kr * (threads / 32) * 4 +
-           (size_t)nctl * (tile_x + n2) * sizeof(int2) +
-           2 * (size_t)stencil_r_window_rows(tile_x, n2, threads, kr) * (n2 + 1) * sizeof(float);
+    const size_t ord = (size_t)((nctl + 7) & ~7) * 2;
+    const size_t per = (size_t)(kRWt + 2 * stencil_r_ninc(nsub)) * 4 +
+                       (size_t)tile_mask_stride(tile_x, n2) * 4 +
+                       (size_t)stencil_r_live_groups(tile_x) * 32;
+    const size_t cent = ((size_t)chunk * n2 * 8 + 15) & ~(size_t)15;
+    return ord + (size_t)chunk * per + cent +
+           2 * (size_t)(4 * groups) * stencil_r_row_stride(n2) * sizeof(float);
+}
+
+// v0c + tx * (v1c - v0c) for the two columns, then the y step: the bilinear
+// step of k_stencil_b (whose packed form computes the same IEEE operations
+// per lane).
+__device__ __forceinline__ float r_bilerp(float lo0, float lo1, float hi0, float hi1, float tx,
+                                          float ty) {
+    const float m0 = fmaf(tx, hi0 - lo0, lo0);
+    const float m1 = fmaf(tx, hi1 - lo1, lo1);
+    return fmaf(ty, m1 - m0, m0);
 }
 
 // One work item = (plane, tile of kp.tile_x rows x all columns); block =
-// item.  Needs (tile_x + 3) * n2 <= KR * blockDim.x and blockDim.x a
-// multiple of 32.  The block first stages what its controls need into
-// shared memory; the control loop then reads nothing else but the corner
-// values at the start of each group.
+// item.  Needs blockDim.x a multiple of 32 and >= kp.rgroups * Ny, and
+// tile_x + 3 <= 4 kp.rgroups.  Threads past rgroups * Ny only help with the
+// staging.
 template <typename S, bool ARGMIN, int KR>
 __device__ __forceinline__ void stencil_r_item(
     const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
     const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask, const KParams& kp,
     const uint16_t* __restrict__ gord, double* part_sum, double* part_max, int16_t* argmin,
     int64_t item, int64_t slot, unsigned char* smem_raw) {
+    static_assert(KR == 4, "a thread owns four window rows of one column");
+    __shared__ int s_nadm;
     const int nctl = kp.nctl;
     const int32_t n1 = kp.g.n[0], n2 = kp.g.n[1];
     const int32_t TX = kp.tile_x;
+    const int32_t G = kp.rgroups;
+    const int32_t CH = kp.rchunk;
     const int T = blockDim.x;
     const int tid = threadIdx.x;
-    const int32_t SB = n2 + 1;  // window row stride (one padding column)
-    const int32_t bsz = stencil_r_window_rows(TX, n2, T, KR) * SB;
-    const int32_t mwq = T >> 5;          // mask words per cell slot
-    const int32_t MWS = KR * mwq;        // mask words per control in shared memory
-    const int32_t TS = tile_mask_stride(TX, n2);  // mask words per control in the tile mask
-    const int32_t NI = stencil_r_ninc(kp.nsub);   // increments per axis in shared memory
-    const int32_t ecs = TX + n2;  // successor entries per control
-    const int32_t RW = kRWt + 2 * NI;    // parameter words per control
+    const int32_t SB = stencil_r_row_stride(n2);  // window row stride in floats
+    const int32_t SB4 = 4 * SB;      // and in bytes
+    const int32_t GL = stencil_r_live_groups(TX);
+    const int32_t TS = tile_mask_stride(TX, n2);
+    const int32_t NI = stencil_r_ninc(kp.nsub);
+    const int32_t RW = kRWt + 2 * NI;
+    const int32_t bsz = 4 * G * SB;  // floats per window buffer
     uint16_t* ord = reinterpret_cast<uint16_t*>(smem_raw);
-    float* wt = reinterpret_cast<float*>(ord + ((nctl + 7) & ~7));  // [nctl][RW]
-    uint32_t* msk = reinterpret_cast<uint32_t*>(wt + nctl * RW);    // [nctl][MWS]
-    // [nctl][ecs]: TX rows (window offset, x fraction), n2 columns (column,
-    // y fraction)
-    int2* ent = reinterpret_cast<int2*>(msk + nctl * MWS);
-    float* Bbuf = reinterpret_cast<float*>(ent + (size_t)nctl * ecs);
+    float* wt = reinterpret_cast<float*>(smem_raw + (size_t)((nctl + 7) & ~7) * 2);  // [CH][RW]
+    uint32_t* msk = reinterpret_cast<uint32_t*>(wt + CH * RW);                        // [CH][TS]
+    int4* rent = reinterpret_cast<int4*>(msk + CH * TS);       // [CH][GL][2]: offsets, fractions
+    int2* cent = reinterpret_cast<int2*>(rent + CH * GL * 2);  // [CH][Ny]
+    float* Bbuf = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(cent) +
+                                           (((size_t)CH * n2 * 8 + 15) & ~(size_t)15));
     const Layout L = make_layout(kp);
     const float cap = kp.p.cap;
     const int64_t P = L.P;
@@ -262,7 +298,6 @@ __device__ __forceinline__ void stencil_r_item(
     const int32_t xt = (int32_t)(item - pl * kp.tiles_x);
     const int32_t x0 = xt * TX;
     const int32_t nr = min(TX, n1 - x0);
-    const int32_t ncell = nr * n2;
     int32_t pq6[4];
     {
         int64_t pp = pl;
@@ -273,239 +308,258 @@ __device__ __forceinline__ void stencil_r_item(
     }
     const uint32_t* prec = recs + (size_t)pl * nctl * kURec;
 
-    // stage the block's per-control data with asynchronous copies, waited
-    // for once below: per control its record's words 0-19 (w[16], tau, tx,
-    // ty, -) and kUNT+16..19 (ox, oy, ok, nsub) as six 16-byte pieces, its
-    // first NI x and y increments, and its mask words (zero past the tile's)
-    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
-    for (int i = tid; i < nctl * 6; i += T) {
-        const int u = i / 6, c = i - u * 6;
-        cp_async16(wt + u * RW + 4 * c, prec + (size_t)u * kURec + (c < 5 ? 4 * c : kUNT + 16));
-    }
-    {
-        const int32_t pieces = NI / 2;  // 16-byte pieces per control: NI/4 for x, NI/4 for y
-        for (int i = tid; i < nctl * pieces; i += T) {
-            const int u = i / pieces, c = i - u * pieces;
-            const int32_t half = NI / 4;
-            const int32_t src = c < half ? kUInc + 4 * c : kUInc + kStencilMaxSub + 4 * (c - half);
-            cp_async16(wt + u * RW + kRWt + 4 * c, prec + (size_t)u * kURec + src);
-        }
-    }
-    {
-        // tile word tw = q * mwq + w (cell slot q, warp w) lands at w * KR + q,
-        // so that a warp's KR words are one vector; words past the tile's are 0
-        const uint32_t* src = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * TS;
-        for (int i = tid; i < nctl * TS; i += T) {
-            const int u = i / TS, tw = i - u * TS;
-            const int32_t q = tw / mwq, w = tw - q * mwq;
-            cp_async4(msk + u * MWS + w * KR + q, src + (size_t)u * TS + tw);
-        }
-        for (int i = tid; i < nctl * MWS; i += T) {
-            const int u = i / MWS, r = i - u * MWS;
-            const int32_t w = r / KR, q = r - w * KR;
-            if (q * mwq + w >= TS) msk[i] = 0u;
-        }
-    }
-    cp_async_commit();
+    // this thread: column j of the window rows 4g .. 4g+3 (act) and of the
+    // tile's cells in those rows (cel)
+    const int32_t g = tid / n2;
+    const int32_t j = tid - g * n2;
+    const bool act = g < G;
+    const bool cel = g < GL;
+    const int wid = tid >> 5, nw = T >> 5;
+    const uint32_t lane = (uint32_t)tid & 31u;
 
-    // this thread's tile cells e = tid + q*T: (row a, column j) packed
+    // the group order; admissible controls first, nadm of them
+    if (tid == 0) s_nadm = nctl;
+    for (int i = tid; i < nctl; i += T) ord[i] = __ldg(gord + (size_t)pl * nctl + i);
+    __syncthreads();
+    for (int i = tid; i < nctl; i += T)
+        if ((ord[i] & kCtlInadmissible) && (i == 0 || !(ord[i - 1] & kCtlInadmissible)))
+            s_nadm = i;
+    __syncthreads();
+    const int nadm = s_nadm;
+
     const uint8_t* occ_h = occ + ((int64_t)pq6[0] * n1 + x0) * n2;
-    float best[KR];
-    int bk[ARGMIN ? KR : 1];
-    int32_t caj[KR];  // a << 16 | j
+    float best[4];
+    int bk[ARGMIN ? 4 : 1];
     uint32_t live = 0;
 #pragma unroll
-    for (int q = 0; q < KR; ++q) {
-        const int32_t e = tid + q * T;
+    for (int q = 0; q < 4; ++q) {
         best[q] = cap;
         if constexpr (ARGMIN) bk[q] = 0x7fffffff;
-        // slots past the tile read cell (0, 0) and are never kept
-        const int32_t a = e < ncell ? e / n2 : 0;
-        caj[q] = e < ncell ? (a << 16) | (e - a * n2) : 0;
-        if (e < ncell && occ_h[e] == 0) live |= 1u << q;
+        const int32_t a = 4 * g + q;
+        if (cel && a < nr && occ_h[a * n2 + j] == 0) live |= 1u << q;
     }
-    // this thread's window slots w = tid + k*T: their offset in the padded
-    // window (slots past the window fall in its scratch rows); bit k of
-    // wlast: slot k is in the last column
-    int32_t wsb[KR];
-    uint32_t wlast = 0;
-#pragma unroll
-    for (int k = 0; k < KR; ++k) {
-        const int32_t w = tid + k * T;
-        const int32_t a = w / n2, j = w - a * n2;
-        wsb[k] = a * SB + j;
-        if (j == n2 - 1) wlast |= 1u << k;
-    }
-    // the warp's mask words in a control's words; its bit is the lane
-    const int32_t mw0 = (tid >> 5) * KR;
-    const uint32_t lane = (uint32_t)tid & 31u;
-    cp_async_wait_all();
-    __syncthreads();
+    const bool jlast = j == n2 - 1;
+    const int32_t wofs = 4 * g * SB + j;  // this thread's first window cell
 
-    // every admissible control's successor entries from its staged
-    // increments: rows (the window offset of the lower corner, the x
-    // fraction), then columns (the lower column, the y fraction).  Many
-    // independent chains per thread, all from shared memory.
-    for (int32_t i = tid; i < nctl * ecs; i += T) {
-        const int u = i / ecs;
-        const int32_t k = i - u * ecs;
-        if (__float_as_uint(wt[u * RW + 22]) == 0u || (k >= nr && k < TX)) continue;
-        const bool row = k < TX;
-        int32_t li;
-        float t;
-        succ_li_t(kp.g, wt + u * RW + kRWt + (row ? 0 : NI), kp.nsub, row,
-                  row ? x0 + k : k - TX, n1, n2, &li, &t);
-        if (row) {
-            const int32_t wbase = x0 + __float_as_int(wt[u * RW + 20]) - 1;
-            ent[i] = make_int2(min(max(li - wbase, 0), nr + 1) * SB, __float_as_int(t));
-        } else {
-            ent[i] = make_int2(min(max(li, 0), n2 - 1), __float_as_int(t));
-        }
-    }
-    __syncthreads();
-    // the increments are spent: rewrite each control's parameter area as
-    // its weights duplicated into FP32 pairs for the packed blend, then the
-    // eight parameter words (each thread its own controls, so no barrier
-    // between reading and writing one)
-    for (int u = tid; u < nctl; u += T) {
-        float* a = wt + u * RW;
-        float w[16], par[8];
+    uint64_t cv[2][16];  // the group's corner values, rows (4g, 4g+1) and (4g+2, 4g+3) paired
+    // corner values of the group that the control at position p starts: the
+    // planes of its record, rows from its x offset
+    auto load_group = [&](int p) {
+        const uint32_t* rec = prec + (size_t)(ord[p] & kCtlMask) * kURec;
+        const int32_t wbase = x0 + (int32_t)__ldg(rec + kUNT + 16) - 1;
+        const S* base[4];
 #pragma unroll
-        for (int c = 0; c < 16; ++c) w[c] = a[c];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) par[c] = a[16 + c];
-#pragma unroll
-        for (int c = 0; c < 16; ++c) { a[2 * c] = w[c]; a[2 * c + 1] = w[c]; }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) a[kRTau + c] = par[c];
-    }
-    __syncthreads();
-
-    static_assert(KR % 2 == 0, "window slots are paired for the packed FMA");
-    uint64_t cv[KR / 2][16];  // the group's corner values, slots 2i and 2i+1 paired
-    // corner values of the group that control uu starts: the planes of its
-    // record, rows from its x offset
-    auto load_group = [&](int uu) {
-        const int u = ord[uu] & 0x7fff;
-        const int32_t wbase = x0 + __float_as_int(wt[u * RW + kROx]) - 1;
-        const uint32_t* rec = prec + (size_t)u * kURec;
-        const S* base[KR];
-#pragma unroll
-        for (int k = 0; k < KR; ++k) {
-            const int32_t a = wsb[k] / SB, j = wsb[k] - a * SB;
-            const int32_t r = min(max(wbase + a, 0), n1 - 1);
+        for (int k = 0; k < 4; ++k) {
+            const int32_t r = min(max(wbase + 4 * g + k, 0), n1 - 1);
             base[k] = Vin + (int64_t)r * n2 + j;
         }
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
             const int64_t off = (int64_t)__ldg(rec + kUNT + c) * P;
-#pragma unroll
-            for (int k = 0; k < KR; k += 2)
-                cv[k / 2][c] = pk2(Conv<S>::ld(base[k] + off), Conv<S>::ld(base[k + 1] + off));
+            cv[0][c] = pk2(Conv<S>::ld(base[0] + off), Conv<S>::ld(base[1] + off));
+            cv[1][c] = pk2(Conv<S>::ld(base[2] + off), Conv<S>::ld(base[3] + off));
         }
     };
-    // the first control starts a group; inadmissible controls come last and
-    // their records' corner planes are never read
-    if (__float_as_uint(wt[(ord[0] & 0x7fff) * RW + kROk]) != 0u) load_group(0);
-    int buf = 0;
-    for (int uu = 0; uu < nctl; ++uu) {
-        const uint32_t ent_u = ord[uu];
-        const int u = (int)(ent_u & 0x7fffu);
-        const float* wu = wt + u * RW;
-        if (__float_as_uint(wu[kROk]) == 0u) {
-            // no cell of the plane admits this control (block-uniform)
-            if constexpr (ARGMIN) {
-#pragma unroll
-                for (int q = 0; q < KR; ++q)
-                    if (best[q] == cap && u < bk[q]) bk[q] = u;
-            }
-            continue;
-        }
-        float* B = Bbuf + buf * bsz;
-        buf ^= 1;
+    if (nadm > 0 && act) load_group(0);
 
-        // phase 1: blend, 16 FMAs per window slot from registers
+    int buf = 0;
+    for (int c0 = 0; c0 < nadm; c0 += CH) {
+        const int ch = min(CH, nadm - c0);
+        // stage the chunk's per-control data, a warp per control: its
+        // record's words 0-19 (w[16], tau, tx, ty, -) and kUNT+16..19 (ox,
+        // oy, ok, nsub) as six 16-byte pieces, its first NI x and y
+        // increments, and its mask words
         {
-            uint64_t acc2[KR / 2];
-#pragma unroll
-            for (int k = 0; k < KR / 2; ++k) acc2[k] = 0ull;
-#pragma unroll
-            for (int c4 = 0; c4 < 4; ++c4) {
-                // (w, w) pairs of corners 4 c4 .. 4 c4 + 3
-                const ulonglong2 wa = reinterpret_cast<const ulonglong2*>(wu)[2 * c4];
-                const ulonglong2 wb = reinterpret_cast<const ulonglong2*>(wu)[2 * c4 + 1];
-#pragma unroll
-                for (int k = 0; k < KR / 2; ++k) {
-                    acc2[k] = fma2(wa.x, cv[k][4 * c4 + 0], acc2[k]);
-                    acc2[k] = fma2(wa.y, cv[k][4 * c4 + 1], acc2[k]);
-                    acc2[k] = fma2(wb.x, cv[k][4 * c4 + 2], acc2[k]);
-                    acc2[k] = fma2(wb.y, cv[k][4 * c4 + 3], acc2[k]);
+            const int32_t pieces = NI / 2, half = NI / 4;
+            const int32_t npc = 6 + pieces + TS / 4;
+            for (int lp = wid; lp < ch; lp += nw) {
+                const int u = ord[c0 + lp] & kCtlMask;
+                const uint32_t* rec = prec + (size_t)u * kURec;
+                const uint32_t* tm = tmask + ((size_t)(pl * kp.tiles_x + xt) * nctl + u) * TS;
+                for (int c = (int)lane; c < npc; c += 32) {
+                    if (c < 6) {
+                        cp_async16(wt + lp * RW + 4 * c, rec + (c < 5 ? 4 * c : kUNT + 16));
+                    } else if (c < 6 + pieces) {
+                        const int32_t k = c - 6;
+                        cp_async16(wt + lp * RW + kRWt + 4 * k,
+                                   rec + (k < half ? kUInc + 4 * k : kUInc + kStencilMaxSub + 4 * (k - half)));
+                    } else {
+                        const int32_t k = c - 6 - pieces;
+                        cp_async16(msk + lp * TS + 4 * k, tm + 4 * k);
+                    }
                 }
             }
-            float acc[KR];
-#pragma unroll
-            for (int k = 0; k < KR / 2; ++k) upk2(acc2[k], acc[2 * k], acc[2 * k + 1]);
-#pragma unroll
-            for (int k = 0; k < KR; ++k) {
-                B[wsb[k]] = acc[k];
-                // the padding column repeats the last one
-                if ((wlast >> k) & 1u) B[wsb[k] + 1] = acc[k];
-            }
+            cp_async_commit();
+            cp_async_wait_all();
         }
-        // the corner values are free now: if the next control starts a new
-        // group, its loads fly during this control's barrier and phase 2
-        if (uu + 1 < nctl && (ord[uu + 1] & kGroupFirst) &&
-            __float_as_uint(wt[(ord[uu + 1] & 0x7fff) * RW + kROk]) != 0u)
-            load_group(uu + 1);
         __syncthreads();
 
-        // phase 2: shift, admissibility, tau, min -- computed for every cell
-        // slot (entries are clamped into the window, dead slots read cell
-        // (0, 0)), kept where the control is admissible.  The mask has no
-        // bit for an occupied cell or a slot past the tile, so it alone
-        // decides; the bilinear step takes the two row lerps as one packed
-        // FMA (the same IEEE operations per lane as k_stencil_b's).
-        const float tau = wu[kRTau];
-        const int2* ri = ent + (size_t)u * ecs;
-        const int2* ci = ri + TX;
-        uint32_t mw[KR];  // the warp's mask words of this control, one vector load
-        {
-            const uint32_t* mu = msk + u * MWS + mw0;
-            if constexpr (KR == 4) {
-                const uint4 m4 = *reinterpret_cast<const uint4*>(mu);
-                mw[0] = m4.x; mw[1] = m4.y; mw[2] = m4.z; mw[3] = m4.w;
-            } else {
-#pragma unroll
-                for (int q = 0; q < KR; ++q) mw[q] = mu[q];
+        // every staged control's successor entries from its increments, a
+        // warp per control and a lane per tile row or column: per live row
+        // group the four rows' window offsets (the lower corner's row from the
+        // window base, in bytes) and x fractions, then per column the lower
+        // column's byte offset and the y fraction
+        for (int lp = wid; lp < ch; lp += nw) {
+            const float* a = wt + lp * RW;
+            const int32_t wbase = x0 + __float_as_int(a[20]) - 1;
+            int32_t* re = reinterpret_cast<int32_t*>(rent + lp * GL * 2);
+            for (int k = (int)lane; k < 4 * GL + n2; k += 32) {
+                const bool row = k < 4 * GL;
+                if (row && k >= nr) {  // a tile row past the plane: no cell reads it
+                    re[(k >> 2) * 8 + (k & 3)] = 0;
+                    re[(k >> 2) * 8 + 4 + (k & 3)] = 0;
+                    continue;
+                }
+                int32_t li;
+                float t;
+                succ_li_t(kp.g, a + kRWt + (row ? 0 : NI), kp.nsub, row, row ? x0 + k : k - 4 * GL,
+                          n1, n2, &li, &t);
+                if (row) {
+                    re[(k >> 2) * 8 + (k & 3)] = min(max(li - wbase, 0), nr + 1) * SB4;
+                    re[(k >> 2) * 8 + 4 + (k & 3)] = __float_as_int(t);
+                } else {
+                    cent[lp * n2 + k - 4 * GL] =
+                        make_int2(min(max(li, 0), n2 - 1) * 4, __float_as_int(t));
+                }
             }
         }
+        __syncthreads();
+        // the increments are spent: rewrite each control's parameter area as
+        // its weights duplicated into FP32 pairs for the packed blend, then the
+        // eight parameter words (each thread its own controls)
+        for (int lp = tid; lp < ch; lp += T) {
+            float* a = wt + lp * RW;
+            float w[16], par[8];
 #pragma unroll
-        for (int q = 0; q < KR; ++q) {
-            // warp-uniform: slots no lane of the warp has a cell in
-            if ((tid & ~31) + q * T >= ncell) break;
-            const int32_t a = caj[q] >> 16, j = caj[q] & 0xffff;
-            const bool adm = (mw[q] >> lane) & 1u;
-            const int2 rr = ri[a];
-            const int2 cc = ci[j];
-            const float tx = __int_as_float(rr.y), ty = __int_as_float(cc.y);
-            const float* p = B + rr.x + cc.x;
-            const uint64_t lo = pk2(p[0], p[1]), hi = pk2(p[SB], p[SB + 1]);
-            float m0, m1;  // v0c + tx * (v1c - v0c) for columns c = 0, 1
-            upk2(fma2(pk2(tx, tx), sub2(hi, lo), lo), m0, m1);
-            const float val = fmaf(ty, m1 - m0, m0);
-            if constexpr (ARGMIN) {
-                const float cvl = adm ? fminf(tau + fminf(val, cap), cap) : cap;
-                // equal values go to the lower table index, which is what
-                // the reference's strict < in table order keeps
-                if (cvl < best[q] || (cvl == best[q] && u < bk[q])) {
-                    best[q] = cvl;
-                    bk[q] = u;
-                }
-            } else {
-                // best <= cap throughout, so min(best, min(tau + min(val,
-                // cap), cap)) is min(best, tau + val) for finite values
-                if (adm) best[q] = fminf(best[q], tau + val);
+            for (int c = 0; c < 16; ++c) w[c] = a[c];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) par[c] = a[16 + c];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) { a[2 * c] = w[c]; a[2 * c + 1] = w[c]; }
+#pragma unroll
+            for (int c = 0; c < 8; ++c) a[kRTau + c] = par[c];
+            const int p1 = c0 + lp + 1;
+            a[kRNext] = __int_as_float((p1 < nadm && (ord[p1] & kGroupFirst)) ? 1 : 0);
+            // bit 0 of a row group's first offset: its four rows are live and
+            // their successor rows consecutive
+            int4* ro = rent + lp * GL * 2;
+            for (int k = 0; k < GL; ++k) {
+                const int4 o = ro[2 * k];
+                const bool cons = 4 * k + 3 < nr && o.y == o.x + SB4 && o.z == o.x + 2 * SB4 &&
+                                  o.w == o.x + 3 * SB4;
+                if (cons) ro[2 * k].x = o.x | 1;
             }
+        }
+        __syncthreads();
+
+        for (int lp = 0; lp < ch; ++lp) {
+            const float* wu = wt + lp * RW;
+            float* B = Bbuf + buf * bsz;
+            buf ^= 1;
+            // phase 1: blend, 16 FMAs per window cell from registers
+            if (act) {
+                uint64_t acc2[2] = {0ull, 0ull};
+#pragma unroll
+                for (int c4 = 0; c4 < 4; ++c4) {
+                    // (w, w) pairs of corners 4 c4 .. 4 c4 + 3
+                    const ulonglong2 wa = reinterpret_cast<const ulonglong2*>(wu)[2 * c4];
+                    const ulonglong2 wb = reinterpret_cast<const ulonglong2*>(wu)[2 * c4 + 1];
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        acc2[k] = fma2(wa.x, cv[k][4 * c4 + 0], acc2[k]);
+                        acc2[k] = fma2(wa.y, cv[k][4 * c4 + 1], acc2[k]);
+                        acc2[k] = fma2(wb.x, cv[k][4 * c4 + 2], acc2[k]);
+                        acc2[k] = fma2(wb.y, cv[k][4 * c4 + 3], acc2[k]);
+                    }
+                }
+                float v0, v1, v2, v3;
+                upk2(acc2[0], v0, v1);
+                upk2(acc2[1], v2, v3);
+                float* bw = B + wofs;
+                bw[0] = v0;
+                bw[SB] = v1;
+                bw[2 * SB] = v2;
+                bw[3 * SB] = v3;
+                if (jlast) {  // the padding column repeats the last one
+                    bw[1] = v0;
+                    bw[SB + 1] = v1;
+                    bw[2 * SB + 1] = v2;
+                    bw[3 * SB + 1] = v3;
+                }
+                // the corner values are free now: if the next control starts a
+                // new group, its loads fly during this control's barrier and
+                // phase 2
+                if (__float_as_int(wu[kRNext]) != 0) load_group(c0 + lp + 1);
+            }
+            __syncthreads();
+
+            // phase 2: shift, admissibility, tau, min for the thread's four
+            // cells -- computed for every row of the group (dead rows read row
+            // 0 and have no mask bit), kept where the control is admissible
+            if (cel) {
+                const float tau = wu[kRTau];
+                const int4 ro = rent[(lp * GL + g) * 2];
+                const int4 rf = rent[(lp * GL + g) * 2 + 1];
+                const int2 cc = cent[lp * n2 + j];
+                const uint4 m4 = *reinterpret_cast<const uint4*>(msk + lp * TS + 4 * wid);
+                const float ty = __int_as_float(cc.y);
+                const float tx[4] = {__int_as_float(rf.x), __int_as_float(rf.y), __int_as_float(rf.z),
+                                     __int_as_float(rf.w)};
+                const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+                const unsigned char* Bc = reinterpret_cast<const unsigned char*>(B) + cc.x;
+                float val[4];
+                if (ro.x & 1) {
+                    // consecutive successor rows: five window rows serve the
+                    // four cells
+                    const unsigned char* p = Bc + (ro.x & ~1);
+                    float v[5][2];
+#pragma unroll
+                    for (int r = 0; r < 5; ++r) {
+                        v[r][0] = *reinterpret_cast<const float*>(p + r * SB4);
+                        v[r][1] = *reinterpret_cast<const float*>(p + r * SB4 + 4);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        val[q] = r_bilerp(v[q][0], v[q][1], v[q + 1][0], v[q + 1][1], tx[q], ty);
+                } else {
+                    const int32_t offs[4] = {ro.x, ro.y, ro.z, ro.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float* p = reinterpret_cast<const float*>(Bc + offs[q]);
+                        val[q] = r_bilerp(p[0], p[1], p[SB], p[SB + 1], tx[q], ty);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const bool adm = (mw[q] >> lane) & 1u;
+                    if constexpr (ARGMIN) {
+                        const int u = ord[c0 + lp] & kCtlMask;
+                        const float cvl = adm ? fminf(tau + fminf(val[q], cap), cap) : cap;
+                        // equal values go to the lower table index, which is
+                        // what the reference's strict < in table order keeps
+                        if (cvl < best[q] || (cvl == best[q] && u < bk[q])) {
+                            best[q] = cvl;
+                            bk[q] = u;
+                        }
+                    } else {
+                        // best <= cap throughout, so min(best, min(tau +
+                        // min(val, cap), cap)) is min(best, tau + val) for
+                        // finite values
+                        if (adm) best[q] = fminf(best[q], tau + val[q]);
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the chunk's shared data is read; the next chunk may stage
+    }
+    if constexpr (ARGMIN) {
+        // controls no cell of the plane admits: ties at the cap go to the
+        // lower table index
+        for (int p = nadm; p < nctl; ++p) {
+            const int u = ord[p] & kCtlMask;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (best[q] == cap && u < bk[q]) bk[q] = u;
         }
     }
 
@@ -513,25 +567,28 @@ __device__ __forceinline__ void stencil_r_item(
     const S* Vp0 = Vin + pl * P + (int64_t)x0 * n2;
     S* Vo0 = Vout + pl * P + (int64_t)x0 * n2;
     double dsum = 0.0, dmax = 0.0;
+    if (cel) {
 #pragma unroll
-    for (int q = 0; q < KR; ++q) {
-        const int32_t e = tid + q * T;
-        if (e >= ncell) break;
-        const S ov = Vp0[e];
-        const float old = (float)Conv<S>::val(ov);
-        const bool lv = (live >> q) & 1u;
-        if constexpr (ARGMIN)
-            argmin[L.rowmajor(x0 + (caj[q] >> 16), caj[q] & 0xffff, pq6[0], pq6[1], pq6[2],
-                              pq6[3])] = lv ? (int16_t)bk[q] : (int16_t)-1;
-        if (lv && (best[q] < old || (kp.relax && old > 0.0f && best[q] != old))) {
-            const S nv = Conv<S>::template st<float>(best[q]);
-            const float nvT = (float)Conv<S>::val(nv);
-            Vo0[e] = nv;
-            const double d = fabs((double)old - (double)nvT);
-            dsum += d;
-            dmax = fmax(dmax, d);
-        } else {
-            Vo0[e] = ov;
+        for (int q = 0; q < 4; ++q) {
+            const int32_t a = 4 * g + q;
+            if (a >= nr) break;
+            const int32_t e = a * n2 + j;
+            const S ov = Vp0[e];
+            const float old = (float)Conv<S>::val(ov);
+            const bool lv = (live >> q) & 1u;
+            if constexpr (ARGMIN)
+                argmin[L.rowmajor(x0 + a, j, pq6[0], pq6[1], pq6[2], pq6[3])] =
+                    lv ? (int16_t)bk[q] : (int16_t)-1;
+            if (lv && (best[q] < old || (kp.relax && old > 0.0f && best[q] != old))) {
+                const S nv = Conv<S>::template st<float>(best[q]);
+                const float nvT = (float)Conv<S>::val(nv);
+                Vo0[e] = nv;
+                const double d = fabs((double)old - (double)nvT);
+                dsum += d;
+                dmax = fmax(dmax, d);
+            } else {
+                Vo0[e] = ov;
+            }
         }
     }
     block_partial_at(dsum, dmax, part_sum, part_max, slot);

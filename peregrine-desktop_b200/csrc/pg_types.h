@@ -20,6 +20,13 @@ constexpr int kBMaxTileCells = 1024;
 // register-resident blend: window cells per block, and per thread
 constexpr int kRMaxWindowHost = 2048;
 constexpr int kRCellsPerThread = 4;
+// register-resident blend: dynamic shared memory a block may take (the
+// sm_100 maximum per block, 227 KB, less 2 KB for the kernels' static
+// shared memory)
+constexpr int kRSmemMax = 225 * 1024;
+// register-resident blend: controls per plane at most (14-bit indices in
+// the group order)
+constexpr int kCtlMaskHost = 0x3fff;
 // Model entries the adjoint differentiates (diagonals of B, A, S, D; q; c).
 constexpr int kNThetaHost = 18;
 
@@ -52,7 +59,10 @@ struct KParams {
     int32_t bblock;   // blend-then-shift: threads per block
     int32_t rtile_x;  // register-resident blend: x rows per block (0: not eligible)
     int32_t rtiles_x; // register-resident blend: blocks per plane
-    int32_t rblock;   // register-resident blend: threads per block
+    int32_t rblock;   // register-resident blend: threads per block (a multiple of 32)
+    int32_t rgroups;  // register-resident blend: row groups of 4 window rows; the
+                      // first rgroups * Ny threads of a block own one column each
+    int32_t rchunk;   // register-resident blend: controls staged in shared memory at once
     int32_t relax;    // 0: V' = min(V, T V), the reference's update; 1: V' = T V except
                       // where V = 0 (target cells, which stay pinned)
     int32_t phase;

@@ -18,12 +18,12 @@ def bench():
     return mod
 
 
-@pytest.mark.parametrize("n1,n2,rows", [(48, 48, 16), (24, 24, 24), (96, 96, 16), (12, 12, 12)])
-def test_tile_rows_follow_the_library_rule(bench, n1, n2, rows):
-    # (rows + 3) * n2 window cells: within 1024 when the 3 extra rows cost at
-    # most a quarter, else within 2048; tiles balanced over the plane
-    assert bench.blend_tile_rows(n1, n2) == rows
-    assert (rows + 3) * n2 <= 2048
+@pytest.mark.parametrize("n1,n2,rows,groups", [(48, 48, 16, 5), (24, 24, 24, 7), (96, 96, 16, 5),
+                                               (12, 12, 12, 4), (40, 48, 8, 3), (10, 192, 5, 2)])
+def test_tile_rows_follow_the_library_rule(bench, n1, n2, rows, groups):
+    # four window rows per row group: rows + 3 <= 4 groups, groups * n2 <= 512
+    assert bench.blend_tiling(n1, n2) == (rows, groups)
+    assert rows + 3 <= 4 * groups and groups * n2 <= 512
 
 
 def test_onchip_model(bench):
@@ -34,9 +34,9 @@ def test_onchip_model(bench):
         grid = Grid()
 
     out = bench.onchip_rooflines(Pr(), 1.0e11, 4, None)
-    win = 19 / 16
-    assert out["tile_rows"] == 16
-    assert abs(out["bytes_per_update"] - (4 * win + 32 + 4 / 32)) < 1e-12
+    win = 4 * 5 / 16
+    assert out["tile_rows"] == 16 and out["row_groups"] == 5
+    assert abs(out["bytes_per_update"] - (4 * win + 20 + 4 / 32)) < 1e-12
     assert abs(out["flops_per_update"] - (2 * (16 * win + 3) + 4)) < 1e-12
 
 
