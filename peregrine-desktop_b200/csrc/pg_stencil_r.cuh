@@ -24,11 +24,13 @@
 //   asynchronous copies (a chunk of controls at a time when they do not all
 //   fit), computes from the increments every control's per-row and
 //   per-column successor corners and fractions, and walks the controls in
-//   group order.  At the first control of a group each thread loads the 16
-//   corner values of its four window cells into registers; for every control
-//   it blends them with the control's 16 weights (16 FMAs per window cell,
-//   two cells per packed fma.rn.f32x2, nothing re-read) into the shared
-//   window; then it shifts: its four cells lie in consecutive rows of one
+//   group order, two per step while both are in one group.  At the first
+//   control of a group each thread loads the 16 corner values of its four
+//   window cells into registers; for every control it blends them with the
+//   control's 16 weights (16 FMAs per window cell, two cells per packed
+//   fma.rn.f32x2, the two controls' chains interleaved, nothing re-read)
+//   into the shared window; one barrier per step; then it shifts: its four
+//   cells lie in consecutive rows of one
 //   column, and the successor rows of consecutive rows are nearly always
 //   consecutive too, so the four bilinear steps read five window rows (ten
 //   values) instead of eight, the column entry once, the row entries and
@@ -212,7 +214,8 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
 // words --, its mask words, its row entries (per live row group: the four
 // rows' window offsets in bytes, then their x fractions) and its column
 // entries (per column: the lower column's byte offset and the y fraction);
-// then two window buffers of 4 G rows of stencil_r_row_stride(Ny) floats.
+// then four window buffers (two controls a step, double-buffered) of 4 G
+// rows of stencil_r_row_stride(Ny) floats.
 // Window row stride in floats: at least Ny + 1 (one padding column), and,
 // when Ny is a multiple of 4, such that rows four apart differ by Ny mod 32
 // banks -- a warp whose lanes straddle two row groups (the end of row 4g,
@@ -245,7 +248,7 @@ __host__ __device__ inline size_t stencil_r_smem(int nctl, int chunk, int tile_x
                        (size_t)stencil_r_live_groups(tile_x) * 32;
     const size_t cent = ((size_t)chunk * n2 * 8 + 15) & ~(size_t)15;
     return ord + (size_t)chunk * per + cent +
-           2 * (size_t)(4 * groups) * stencil_r_row_stride(n2) * sizeof(float);
+           4 * (size_t)(4 * groups) * stencil_r_row_stride(n2) * sizeof(float);
 }
 
 // v0c + tx * (v1c - v0c) for the two columns, then the y step: the bilinear
@@ -256,6 +259,85 @@ __device__ __forceinline__ float r_bilerp(float lo0, float lo1, float hi0, float
     const float m0 = fmaf(tx, hi0 - lo0, lo0);
     const float m1 = fmaf(tx, hi1 - lo1, lo1);
     return fmaf(ty, m1 - m0, m0);
+}
+
+// The four blended window values of a thread (rows 4g .. 4g+3 of its
+// column, two packed pairs) into the window at bw, and into the padding
+// column when the thread's column is the last.
+__device__ __forceinline__ void r_store_window(float* bw, const uint64_t* a2, int32_t SB, bool jlast) {
+    float v0, v1, v2, v3;
+    upk2(a2[0], v0, v1);
+    upk2(a2[1], v2, v3);
+    bw[0] = v0;
+    bw[SB] = v1;
+    bw[2 * SB] = v2;
+    bw[3 * SB] = v3;
+    if (jlast) {
+        bw[1] = v0;
+        bw[SB + 1] = v1;
+        bw[2 * SB + 1] = v2;
+        bw[3 * SB + 1] = v3;
+    }
+}
+
+// Phase 2 of one control for a thread's four cells (rows 4g .. 4g+3 of its
+// column): shift, admissibility, tau, min -- computed for every row of the
+// group (dead rows read row 0 and have no mask bit), kept where the control
+// is admissible.  wu: the control's parameter area; B: its window; ro: its
+// row group's entries (offsets, then fractions); cc: its column entry; mk:
+// the warp's four mask words; u: its table index (argmin only).
+template <bool ARGMIN>
+__device__ __forceinline__ void r_shift(const float* wu, const float* B, const int4* ro2,
+                                        const int2 cc, const uint32_t* mk, int32_t SB4,
+                                        uint32_t lane, float cap, int u, float* best, int* bk) {
+    const float tau = wu[kRTau];
+    const int4 ro = ro2[0];
+    const int4 rf = ro2[1];
+    const uint4 m4 = *reinterpret_cast<const uint4*>(mk);
+    const float ty = __int_as_float(cc.y);
+    const float tx[4] = {__int_as_float(rf.x), __int_as_float(rf.y), __int_as_float(rf.z),
+                         __int_as_float(rf.w)};
+    const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+    const unsigned char* Bc = reinterpret_cast<const unsigned char*>(B) + cc.x;
+    float val[4];
+    if (ro.x & 1) {
+        // consecutive successor rows: five window rows serve the four cells
+        const unsigned char* p = Bc + (ro.x & ~1);
+        float v[5][2];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            v[r][0] = *reinterpret_cast<const float*>(p + r * SB4);
+            v[r][1] = *reinterpret_cast<const float*>(p + r * SB4 + 4);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            val[q] = r_bilerp(v[q][0], v[q][1], v[q + 1][0], v[q + 1][1], tx[q], ty);
+    } else {
+        const int32_t offs[4] = {ro.x, ro.y, ro.z, ro.w};
+        const int32_t SB = SB4 >> 2;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float* p = reinterpret_cast<const float*>(Bc + offs[q]);
+            val[q] = r_bilerp(p[0], p[1], p[SB], p[SB + 1], tx[q], ty);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const bool adm = (mw[q] >> lane) & 1u;
+        if constexpr (ARGMIN) {
+            const float cvl = adm ? fminf(tau + fminf(val[q], cap), cap) : cap;
+            // equal values go to the lower table index, which is what the
+            // reference's strict < in table order keeps
+            if (cvl < best[q] || (cvl == best[q] && u < bk[q])) {
+                best[q] = cvl;
+                bk[q] = u;
+            }
+        } else {
+            // best <= cap throughout, so min(best, min(tau + min(val, cap),
+            // cap)) is min(best, tau + val) for finite values
+            if (adm) best[q] = fminf(best[q], tau + val[q]);
+        }
+    }
 }
 
 // One work item = (plane, tile of kp.tile_x rows x all columns); block =
@@ -452,103 +534,86 @@ __device__ __forceinline__ void stencil_r_item(
         }
         __syncthreads();
 
-        for (int lp = 0; lp < ch; ++lp) {
-            const float* wu = wt + lp * RW;
-            float* B = Bbuf + buf * bsz;
+        // the controls two at a time (one barrier per pair) while the second
+        // stays in the first's corner group, else one: blend into the pair's
+        // two window buffers -- the two FMA chains of each control
+        // interleaved, four independent chains per thread --, one barrier,
+        // then shift both
+        int lp = 0;
+        while (lp < ch) {
+            const bool two = lp + 1 < ch && __float_as_int(wt[lp * RW + kRNext]) == 0;
+            const float* wa = wt + lp * RW;
+            const float* wb = wa + RW;
+            float* BA = Bbuf + (2 * buf) * bsz;
+            float* BB = BA + bsz;
             buf ^= 1;
-            // phase 1: blend, 16 FMAs per window cell from registers
             if (act) {
-                uint64_t acc2[2] = {0ull, 0ull};
+                if (two) {
+                    uint64_t a2[2] = {0ull, 0ull}, b2[2] = {0ull, 0ull};
 #pragma unroll
-                for (int c4 = 0; c4 < 4; ++c4) {
-                    // (w, w) pairs of corners 4 c4 .. 4 c4 + 3
-                    const ulonglong2 wa = reinterpret_cast<const ulonglong2*>(wu)[2 * c4];
-                    const ulonglong2 wb = reinterpret_cast<const ulonglong2*>(wu)[2 * c4 + 1];
+                    for (int c4 = 0; c4 < 4; ++c4) {
+                        // (w, w) pairs of corners 4 c4 .. 4 c4 + 3
+                        const ulonglong2 pa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4];
+                        const ulonglong2 qa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4 + 1];
+                        const ulonglong2 pb = reinterpret_cast<const ulonglong2*>(wb)[2 * c4];
+                        const ulonglong2 qb = reinterpret_cast<const ulonglong2*>(wb)[2 * c4 + 1];
 #pragma unroll
-                    for (int k = 0; k < 2; ++k) {
-                        acc2[k] = fma2(wa.x, cv[k][4 * c4 + 0], acc2[k]);
-                        acc2[k] = fma2(wa.y, cv[k][4 * c4 + 1], acc2[k]);
-                        acc2[k] = fma2(wb.x, cv[k][4 * c4 + 2], acc2[k]);
-                        acc2[k] = fma2(wb.y, cv[k][4 * c4 + 3], acc2[k]);
+                        for (int k = 0; k < 2; ++k) {
+                            a2[k] = fma2(pa.x, cv[k][4 * c4 + 0], a2[k]);
+                            b2[k] = fma2(pb.x, cv[k][4 * c4 + 0], b2[k]);
+                        }
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            a2[k] = fma2(pa.y, cv[k][4 * c4 + 1], a2[k]);
+                            b2[k] = fma2(pb.y, cv[k][4 * c4 + 1], b2[k]);
+                        }
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            a2[k] = fma2(qa.x, cv[k][4 * c4 + 2], a2[k]);
+                            b2[k] = fma2(qb.x, cv[k][4 * c4 + 2], b2[k]);
+                        }
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            a2[k] = fma2(qa.y, cv[k][4 * c4 + 3], a2[k]);
+                            b2[k] = fma2(qb.y, cv[k][4 * c4 + 3], b2[k]);
+                        }
                     }
+                    r_store_window(BA + wofs, a2, SB, jlast);
+                    r_store_window(BB + wofs, b2, SB, jlast);
+                } else {
+                    uint64_t a2[2] = {0ull, 0ull};
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4) {
+                        const ulonglong2 pa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4];
+                        const ulonglong2 qa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4 + 1];
+#pragma unroll
+                        for (int k = 0; k < 2; ++k) {
+                            a2[k] = fma2(pa.x, cv[k][4 * c4 + 0], a2[k]);
+                            a2[k] = fma2(pa.y, cv[k][4 * c4 + 1], a2[k]);
+                            a2[k] = fma2(qa.x, cv[k][4 * c4 + 2], a2[k]);
+                            a2[k] = fma2(qa.y, cv[k][4 * c4 + 3], a2[k]);
+                        }
+                    }
+                    r_store_window(BA + wofs, a2, SB, jlast);
                 }
-                float v0, v1, v2, v3;
-                upk2(acc2[0], v0, v1);
-                upk2(acc2[1], v2, v3);
-                float* bw = B + wofs;
-                bw[0] = v0;
-                bw[SB] = v1;
-                bw[2 * SB] = v2;
-                bw[3 * SB] = v3;
-                if (jlast) {  // the padding column repeats the last one
-                    bw[1] = v0;
-                    bw[SB + 1] = v1;
-                    bw[2 * SB + 1] = v2;
-                    bw[3 * SB + 1] = v3;
-                }
-                // the corner values are free now: if the next control starts a
-                // new group, its loads fly during this control's barrier and
-                // phase 2
-                if (__float_as_int(wu[kRNext]) != 0) load_group(c0 + lp + 1);
+                // the corner values are free now: if the control after this
+                // step starts a new group, its loads fly during the barrier
+                // and the shifts
+                const int last = two ? lp + 1 : lp;
+                if (__float_as_int(wt[last * RW + kRNext]) != 0) load_group(c0 + last + 1);
             }
             __syncthreads();
-
-            // phase 2: shift, admissibility, tau, min for the thread's four
-            // cells -- computed for every row of the group (dead rows read row
-            // 0 and have no mask bit), kept where the control is admissible
             if (cel) {
-                const float tau = wu[kRTau];
-                const int4 ro = rent[(lp * GL + g) * 2];
-                const int4 rf = rent[(lp * GL + g) * 2 + 1];
-                const int2 cc = cent[lp * n2 + j];
-                const uint4 m4 = *reinterpret_cast<const uint4*>(msk + lp * TS + 4 * wid);
-                const float ty = __int_as_float(cc.y);
-                const float tx[4] = {__int_as_float(rf.x), __int_as_float(rf.y), __int_as_float(rf.z),
-                                     __int_as_float(rf.w)};
-                const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
-                const unsigned char* Bc = reinterpret_cast<const unsigned char*>(B) + cc.x;
-                float val[4];
-                if (ro.x & 1) {
-                    // consecutive successor rows: five window rows serve the
-                    // four cells
-                    const unsigned char* p = Bc + (ro.x & ~1);
-                    float v[5][2];
-#pragma unroll
-                    for (int r = 0; r < 5; ++r) {
-                        v[r][0] = *reinterpret_cast<const float*>(p + r * SB4);
-                        v[r][1] = *reinterpret_cast<const float*>(p + r * SB4 + 4);
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        val[q] = r_bilerp(v[q][0], v[q][1], v[q + 1][0], v[q + 1][1], tx[q], ty);
-                } else {
-                    const int32_t offs[4] = {ro.x, ro.y, ro.z, ro.w};
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float* p = reinterpret_cast<const float*>(Bc + offs[q]);
-                        val[q] = r_bilerp(p[0], p[1], p[SB], p[SB + 1], tx[q], ty);
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const bool adm = (mw[q] >> lane) & 1u;
-                    if constexpr (ARGMIN) {
-                        const int u = ord[c0 + lp] & kCtlMask;
-                        const float cvl = adm ? fminf(tau + fminf(val[q], cap), cap) : cap;
-                        // equal values go to the lower table index, which is
-                        // what the reference's strict < in table order keeps
-                        if (cvl < best[q] || (cvl == best[q] && u < bk[q])) {
-                            best[q] = cvl;
-                            bk[q] = u;
-                        }
-                    } else {
-                        // best <= cap throughout, so min(best, min(tau +
-                        // min(val, cap), cap)) is min(best, tau + val) for
-                        // finite values
-                        if (adm) best[q] = fminf(best[q], tau + val[q]);
-                    }
-                }
+                r_shift<ARGMIN>(wa, BA, rent + lp * GL * 2 + 2 * g,
+                                cent[lp * n2 + j], msk + lp * TS + 4 * wid, SB4, lane, cap,
+                                ARGMIN ? (int)(ord[c0 + lp] & kCtlMask) : 0, best, bk);
+                if (two)
+                    r_shift<ARGMIN>(wb, BB, rent + (lp + 1) * GL * 2 + 2 * g,
+                                    cent[(lp + 1) * n2 + j], msk + (lp + 1) * TS + 4 * wid, SB4,
+                                    lane, cap, ARGMIN ? (int)(ord[c0 + lp + 1] & kCtlMask) : 0,
+                                    best, bk);
             }
+            lp += two ? 2 : 1;
         }
         __syncthreads();  // the chunk's shared data is read; the next chunk may stage
     }

@@ -109,6 +109,33 @@ def test_adjoint_on_more_cells_than_one_launch_wave(og):
     assert err.max() <= REF_TOL, dict(zip(ag.THETA_NAMES, err))
 
 
+def test_adjoint_on_the_24x24x16x9x9x9_grid_with_125_controls(og):
+    """The config-0 grid (6.7M cells) with the 125 controls of the benchmark
+    ({-1, -0.5, 0, 0.5, 1}^3): the GPU adjoint against the CPU FP64 reference
+    run on the same converged table and policy, within 1e-4 of max |g|."""
+    pr = Problem("small", seed=0, control_set="cube5")
+    spec = ag.SolveSpec.from_problem(pr, iters=6000, tol=1e-6)
+    th0 = ag.theta_of(spec.model)
+    states = ag.start_states(spec.grid, pr.occ, 4096, seed=3)
+    idx, w = ag.interp_weights(spec.grid, states)
+    c = np.zeros(pr.ncells, np.float64)
+    np.add.at(c, idx.ravel(), (w / len(states)).ravel())
+    V, _, ctx = ag.solve(spec, th0, keep=True)
+    try:
+        g, ares = ctx.adjoint(c.astype(np.float32))
+        _, _, pol = ctx.sweep(phase=0, kernel=_lib.KERNEL_STENCIL, argmin=True)
+    finally:
+        ctx.close()
+    g_ = og.copy_struct(spec.grid, og.OGrid)
+    m_ = og.copy_struct(spec.model, og.OModel)
+    p_ = og.copy_struct(spec.params, og.OParams)
+    g_ref, _, nact = og.adjoint_grad_f64(V.astype(np.float64), pol, pr.occ, g_, m_, pr.ctl, p_, c,
+                                         iters=20000, tol=1e-9)
+    assert abs(nact - ares.active_cells) <= 0.001 * nact
+    err = np.abs(g - g_ref) / np.max(np.abs(g_ref))
+    assert err.max() <= REF_TOL, dict(zip(ag.THETA_NAMES, err))
+
+
 def test_autograd_function_matches_the_direct_call(setup):
     s = setup
     theta = torch.tensor(s["th0"], requires_grad=True)
