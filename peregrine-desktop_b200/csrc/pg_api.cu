@@ -200,8 +200,9 @@ int ensure_values(pg_ctx* ctx, int storage) {
 // warps per SM, else the cheapest.  rows < 0, or a tiling that cannot run,
 // leaves it at 0 (not eligible).  The controls a block stages at once
 // (rchunk) are all of them when they fit the shared memory that the blocks
-// the registers allow on an SM share (228 KB, less 1 KB reserved and 1 KB of
-// static shared memory per block), else as many as fit, with fewer blocks per SM only when fewer than 16
+// the registers allow on an SM share (228 KB, less 1 KB reserved and the
+// static shared memory per block, checked with the occupancy calculator),
+// else as many as fit, with fewer blocks per SM only when fewer than 16
 // would fit.
 namespace {
 struct RTile {
@@ -251,25 +252,34 @@ void r_tiling(pg::KParams& kp, int32_t rows) {
             if (better(c, pick)) pick = c;
         }
     }
-    if (pick.tx == 0) return;
+    // the packed row entries hold window byte offsets in 16 bits
+    if (pick.tx == 0 || (int64_t)16 * pick.groups * pg::stencil_r_row_stride_host(n2) > 0xffff) return;
     kp.rtile_x = pick.tx;
     kp.rtiles_x = (n1 + pick.tx - 1) / pick.tx;
     kp.rgroups = pick.groups;
     kp.rblock = pick.block;
-    // controls staged at once: all of them if the blocks that the registers
-    // allow on an SM (up to two) fit in its shared memory, else all that fit
-    // one block per SM, else as many as fit
+    // controls staged at once: as many as fit the blocks that the registers
+    // allow on an SM (up to four), with fewer blocks only when fewer than 16
+    // controls would fit
     const size_t per = pg::stencil_r_ctl_smem_bytes(kp, pick.tx);
     kp.rchunk = 1;
-    const size_t fixed = pg::stencil_r_smem_bytes(kp) - per + 16;
+    const size_t fixed = pg::stencil_r_smem_bytes(kp) - per + 32;  // + the areas' rounding
     const int bps = std::min(4, 512 / pick.block);
+    // a chunk's y increments are staged into the window buffers
+    const int64_t ybuf = (int64_t)16 * pick.groups * pg::stencil_r_row_stride_host(n2) /
+                         std::max(1, pg::stencil_r_ninc_host(kp.nsub));
     int32_t chunk = 0;
     for (int b = bps; b >= 1; --b) {
-        // 228 KB per SM; per block 1 KB reserved and up to 1 KB of static
-        // shared memory
-        const size_t lim = std::min<size_t>((size_t)pg::kRSmemMax, ((size_t)228 / b - 2) * 1024);
-        const int64_t c = lim > fixed ? (int64_t)((lim - fixed) / per) : 0;
-        chunk = (int32_t)std::min<int64_t>(c, kp.nctl);
+        // 228 KB per SM less 1 KB reserved per block; the occupancy
+        // calculator has the last word (the kernel's static shared memory)
+        const size_t lim = std::min<size_t>((size_t)pg::kRSmemMax, 228 * 1024 / b - 1024);
+        int64_t c = lim > fixed ? (int64_t)((lim - fixed) / per) : 0;
+        c = std::min<int64_t>({c, (int64_t)kp.nctl, ybuf});
+        for (; c >= 1; --c) {
+            kp.rchunk = (int32_t)c;
+            if (pg::stencil_r_blocks_per_sm(pick.block, pg::stencil_r_smem_bytes(kp)) >= b) break;
+        }
+        chunk = (int32_t)std::max<int64_t>(c, 0);
         // as many blocks per SM as the registers allow, while a block still
         // stages a useful number of controls at once
         if (chunk >= std::min(kp.nctl, 16)) break;

@@ -1132,8 +1132,9 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
     KParams kr = kp;
     kr.tile_x = kp.rtile_x;
     kr.tiles_x = kp.rtiles_x;
-    const int64_t blocks = kp.nplanes * kp.rtiles_x;
-    if (blocks > sb.nparts || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    // one block per plane sweeps all its tiles; one residual partial per tile
+    const int64_t parts = kp.nplanes * kp.rtiles_x;
+    if (parts > sb.nparts || kp.nplanes > 0x7fffffffLL) return cudaErrorInvalidValue;
     const size_t smem = stencil_r_smem_bytes(kp);
     if (smem > (size_t)kRSmemMax) return cudaErrorInvalidValue;
     static std::atomic<uint64_t> attr_set{0};
@@ -1144,11 +1145,11 @@ static cudaError_t stencil_r_t(const void* Vin, void* Vout, const uint8_t* occ,
         if (e != cudaSuccess) return e;
         attr_set.fetch_or(attr_bit);
     }
-    k_stencil_r<S, ARGMIN, KR><<<(unsigned)blocks, kp.rblock, smem, st>>>(
+    k_stencil_r<S, ARGMIN, KR><<<(unsigned)kp.nplanes, kp.rblock, smem, st>>>(
         (const S*)Vin, (S*)Vout, occ, recs, tmask, kr, gord, sb.part_sum, sb.part_max, argmin);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, blocks, sb.out);
+    k_reduce_parts<<<1, 1024, 0, st>>>(sb.part_sum, sb.part_max, parts, sb.out);
     *launches += 2;
     return cudaGetLastError();
 }
@@ -1241,8 +1242,36 @@ bool stencil_r_shape_ok(const KParams& kp) {
            kp.rblock <= RShape<kRCellsPerThread>::kMaxThreads && kp.rblock % 32 == 0 &&
            kp.rgroups > 0 && (int64_t)kp.rgroups * n2 <= kp.rblock &&
            kp.rtile_x + 3 <= 4 * kp.rgroups && kp.rchunk > 0 && kp.rchunk <= kp.nctl &&
+           // window byte offsets fit 16 bits (the packed row entries)
+           (int64_t)16 * kp.rgroups * stencil_r_row_stride(n2) <= 0xffff &&
+           // the chunk's y increments fit the window buffers
+           (int64_t)kp.rchunk * stencil_r_ninc(kp.nsub) <=
+               (int64_t)16 * kp.rgroups * stencil_r_row_stride(n2) &&
            kp.nctl <= (int)kCtlMask && kp.nsub <= kStencilMaxSub && n2 >= 1 && n2 <= 0xffff;
 }
+
+int stencil_r_blocks_per_sm(int threads, size_t smem) {
+    static std::atomic<uint64_t> attr_set{0};
+    const uint64_t attr_bit = device_bit();
+    if (!(attr_set.load() & attr_bit)) {
+        if (cudaFuncSetAttribute(k_stencil_r<float, false, kRCellsPerThread>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kRSmemMax) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        attr_set.fetch_or(attr_bit);
+    }
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stencil_r<float, false, kRCellsPerThread>,
+                                                      threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return nb;
+}
+
+int32_t stencil_r_row_stride_host(int32_t n2) { return stencil_r_row_stride(n2); }
+int32_t stencil_r_ninc_host(int nsub) { return stencil_r_ninc(nsub); }
 
 size_t stencil_r_ctl_smem_bytes(const KParams& kp, int32_t tile_x) {
     return stencil_r_ctl_bytes(tile_x, kp.g.n[1], kp.nsub);

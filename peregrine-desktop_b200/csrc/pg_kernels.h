@@ -68,6 +68,13 @@ size_t stencil_r_smem_bytes(const KParams& kp);
 // whether kp's register-resident tiling (rtile_x, rgroups, rblock, rchunk)
 // is one k_stencil_r can run
 bool stencil_r_shape_ok(const KParams& kp);
+// resident blocks per SM of k_stencil_r (FP32) with this block size and
+// dynamic shared memory, on the current device (0 when it cannot run)
+int stencil_r_blocks_per_sm(int threads, size_t smem);
+// k_stencil_r's window row stride (floats) for Ny = n2, and its increments
+// staged per control and axis for nsub substeps
+int32_t stencil_r_row_stride_host(int32_t n2);
+int32_t stencil_r_ninc_host(int nsub);
 // shared memory one staged control takes in a k_stencil_r block of tile_x rows
 size_t stencil_r_ctl_smem_bytes(const KParams& kp, int32_t tile_x);
 size_t stencil_tmask_bytes(const KParams& kp);

@@ -205,17 +205,6 @@ __global__ void k_stencil_tmask(const uint32_t* __restrict__ mask, KParams kp, i
     }
 }
 
-// Shared memory of one k_stencil_r block: the plane's group order (all
-// controls); per staged control a parameter area of kRWt + 2 NI words --
-// staged as its record's weights, tau, offsets, admissibility and substeps
-// (24 words) and its substep position increments (x, then y, NI words
-// each), and once the successor entries are made, rewritten as the 16
-// weights each duplicated into an FP32 pair (32 words) and 8 parameter
-// words --, its mask words, its row entries (per live row group: the four
-// rows' window offsets in bytes, then their x fractions) and its column
-// entries (per column: the lower column's byte offset and the y fraction);
-// then four window buffers (two controls a step, double-buffered) of 4 G
-// rows of stencil_r_row_stride(Ny) floats.
 // Window row stride in floats: at least Ny + 1 (one padding column), and,
 // when Ny is a multiple of 4, such that rows four apart differ by Ny mod 32
 // banks -- a warp whose lanes straddle two row groups (the end of row 4g,
@@ -226,28 +215,38 @@ __host__ __device__ inline int32_t stencil_r_row_stride(int32_t n2) {
         while (((4 * sb - n2) & 31) != 0) ++sb;
     return sb;
 }
-constexpr int kRWt = 24;  // as staged: w[16], tau, tx, ty, -, ox, oy, ok, nsub
-// as rewritten: (w, w) pairs in words 0-31, then tau, tx, ty, next, ox, oy,
-// ok, nsub; next = 1 when the following control starts a new group
-constexpr int kRTau = 32, kRNext = 35;
-// x and y increments per control: at least 8 each, so that the parameter
-// area holds the rewritten 40 words
-__host__ __device__ inline int32_t stencil_r_ninc(int nsub) {
-    const int32_t n = (nsub + 3) & ~3;
-    return n > 8 ? n : 8;
-}
+
+// Shared memory of one k_stencil_r block: the plane's group order (all
+// controls); per staged control a parameter area of kRInc + NI words --
+// the 16 weights, each duplicated into an FP32 pair for the packed blend
+// (words 0-31: staged raw into words 16-31, then spread), tau, tx, ty,
+// next, ox, oy, ok, nsub (words 32-39; next = 1 when the following control
+// starts a new corner group), and its x substep position increments (NI
+// words from word 40) --, its mask words for the current tile,
+// its row entries for the current tile (per live row group: the four rows'
+// x fractions, and their window offsets in bytes packed two to a word, bit
+// 0 of the first set when the four successor rows are consecutive) and its
+// column entries (per
+// column: the lower column's byte offset and the y fraction); then four
+// window buffers (two controls a step, double-buffered) of 4 G rows of
+// stencil_r_row_stride(Ny) floats.  The y increments, needed once per plane
+// for the column entries, are staged into the window buffers (NI words per
+// control), which are idle until the first blend.
+constexpr int kRTau = 32, kRNext = 35, kROx = 36, kRInc = 40;
+__host__ __device__ inline int32_t stencil_r_ninc(int nsub) { return (nsub + 3) & ~3; }
 __host__ __device__ inline size_t stencil_r_ctl_bytes(int tile_x, int n2, int nsub) {
-    return (size_t)(kRWt + 2 * stencil_r_ninc(nsub)) * 4 + (size_t)tile_mask_stride(tile_x, n2) * 4 +
-           (size_t)stencil_r_live_groups(tile_x) * 32 + (size_t)n2 * 8;
+    return (size_t)(kRInc + stencil_r_ninc(nsub)) * 4 + (size_t)tile_mask_stride(tile_x, n2) * 4 +
+           (size_t)stencil_r_live_groups(tile_x) * 24 + (size_t)n2 * 8;
 }
 __host__ __device__ inline size_t stencil_r_smem(int nctl, int chunk, int tile_x, int n2, int groups,
                                                  int nsub) {
     const size_t ord = (size_t)((nctl + 7) & ~7) * 2;
-    const size_t per = (size_t)(kRWt + 2 * stencil_r_ninc(nsub)) * 4 +
+    const size_t per = (size_t)(kRInc + stencil_r_ninc(nsub)) * 4 +
                        (size_t)tile_mask_stride(tile_x, n2) * 4 +
-                       (size_t)stencil_r_live_groups(tile_x) * 32;
+                       (size_t)stencil_r_live_groups(tile_x) * 16;
+    const size_t rofs = ((size_t)chunk * stencil_r_live_groups(tile_x) * 8 + 15) & ~(size_t)15;
     const size_t cent = ((size_t)chunk * n2 * 8 + 15) & ~(size_t)15;
-    return ord + (size_t)chunk * per + cent +
+    return ord + (size_t)chunk * per + rofs + cent +
            4 * (size_t)(4 * groups) * stencil_r_row_stride(n2) * sizeof(float);
 }
 
@@ -283,26 +282,26 @@ __device__ __forceinline__ void r_store_window(float* bw, const uint64_t* a2, in
 // Phase 2 of one control for a thread's four cells (rows 4g .. 4g+3 of its
 // column): shift, admissibility, tau, min -- computed for every row of the
 // group (dead rows read row 0 and have no mask bit), kept where the control
-// is admissible.  wu: the control's parameter area; B: its window; ro: its
-// row group's entries (offsets, then fractions); cc: its column entry; mk:
-// the warp's four mask words; u: its table index (argmin only).
+// is admissible.  wu: the control's parameter area; B: its window; rt, rp:
+// its row group's x fractions and packed window offsets; cc: its column
+// entry; mk: the warp's four mask words; u: its table index (argmin only).
 template <bool ARGMIN>
-__device__ __forceinline__ void r_shift(const float* wu, const float* B, const int4* ro2,
-                                        const int2 cc, const uint32_t* mk, int32_t SB4,
-                                        uint32_t lane, float cap, int u, float* best, int* bk) {
+__device__ __forceinline__ void r_shift(const float* wu, const float* B, const float4* rt,
+                                        const uint2* rp, const int2 cc, const uint32_t* mk,
+                                        int32_t SB4, uint32_t lane, float cap, int u, float* best,
+                                        int* bk) {
     const float tau = wu[kRTau];
-    const int4 ro = ro2[0];
-    const int4 rf = ro2[1];
+    const uint2 ro = *rp;
+    const float4 rf = *rt;
     const uint4 m4 = *reinterpret_cast<const uint4*>(mk);
     const float ty = __int_as_float(cc.y);
-    const float tx[4] = {__int_as_float(rf.x), __int_as_float(rf.y), __int_as_float(rf.z),
-                         __int_as_float(rf.w)};
+    const float tx[4] = {rf.x, rf.y, rf.z, rf.w};
     const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
     const unsigned char* Bc = reinterpret_cast<const unsigned char*>(B) + cc.x;
     float val[4];
-    if (ro.x & 1) {
+    if (ro.x & 1u) {
         // consecutive successor rows: five window rows serve the four cells
-        const unsigned char* p = Bc + (ro.x & ~1);
+        const unsigned char* p = Bc + (ro.x & 0xfffeu);
         float v[5][2];
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
@@ -313,7 +312,7 @@ __device__ __forceinline__ void r_shift(const float* wu, const float* B, const i
         for (int q = 0; q < 4; ++q)
             val[q] = r_bilerp(v[q][0], v[q][1], v[q + 1][0], v[q + 1][1], tx[q], ty);
     } else {
-        const int32_t offs[4] = {ro.x, ro.y, ro.z, ro.w};
+        const uint32_t offs[4] = {ro.x & 0xffffu, ro.x >> 16, ro.y & 0xffffu, ro.y >> 16};
         const int32_t SB = SB4 >> 2;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -340,16 +339,19 @@ __device__ __forceinline__ void r_shift(const float* wu, const float* B, const i
     }
 }
 
-// One work item = (plane, tile of kp.tile_x rows x all columns); block =
-// item.  Needs blockDim.x a multiple of 32 and >= kp.rgroups * Ny, and
-// tile_x + 3 <= 4 kp.rgroups.  Threads past rgroups * Ny only help with the
-// staging.
+// The tiles [t0, t1) of plane pl (tiles of kp.tile_x rows x all columns);
+// their residual partials go to slots slot0, slot0 + 1, ...  Needs
+// blockDim.x a multiple of 32 and >= kp.rgroups * Ny, and tile_x + 3 <=
+// 4 kp.rgroups.  Threads past rgroups * Ny only help with the staging.  When
+// one chunk holds every admissible control, the controls' parameters, the
+// column entries and the duplicated weights are made once for all the tiles;
+// per tile only the mask words and the row entries change.
 template <typename S, bool ARGMIN, int KR>
-__device__ __forceinline__ void stencil_r_item(
+__device__ __forceinline__ void stencil_r_plane(
     const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
     const uint32_t* __restrict__ recs, const uint32_t* __restrict__ tmask, const KParams& kp,
     const uint16_t* __restrict__ gord, double* part_sum, double* part_max, int16_t* argmin,
-    int64_t item, int64_t slot, unsigned char* smem_raw) {
+    int64_t pl, int32_t t0, int32_t t1, int64_t slot0, unsigned char* smem_raw) {
     static_assert(KR == 4, "a thread owns four window rows of one column");
     __shared__ int s_nadm;
     const int nctl = kp.nctl;
@@ -360,26 +362,23 @@ __device__ __forceinline__ void stencil_r_item(
     const int T = blockDim.x;
     const int tid = threadIdx.x;
     const int32_t SB = stencil_r_row_stride(n2);  // window row stride in floats
-    const int32_t SB4 = 4 * SB;      // and in bytes
+    const int32_t SB4 = 4 * SB;                   // and in bytes
     const int32_t GL = stencil_r_live_groups(TX);
     const int32_t TS = tile_mask_stride(TX, n2);
     const int32_t NI = stencil_r_ninc(kp.nsub);
-    const int32_t RW = kRWt + 2 * NI;
+    const int32_t RW = kRInc + NI;
     const int32_t bsz = 4 * G * SB;  // floats per window buffer
     uint16_t* ord = reinterpret_cast<uint16_t*>(smem_raw);
     float* wt = reinterpret_cast<float*>(smem_raw + (size_t)((nctl + 7) & ~7) * 2);  // [CH][RW]
     uint32_t* msk = reinterpret_cast<uint32_t*>(wt + CH * RW);                        // [CH][TS]
-    int4* rent = reinterpret_cast<int4*>(msk + CH * TS);       // [CH][GL][2]: offsets, fractions
-    int2* cent = reinterpret_cast<int2*>(rent + CH * GL * 2);  // [CH][Ny]
+    float4* rtx = reinterpret_cast<float4*>(msk + CH * TS);  // [CH][GL]: x fractions
+    uint2* rofs = reinterpret_cast<uint2*>(rtx + CH * GL);    // [CH][GL]: packed offsets
+    int2* cent = reinterpret_cast<int2*>(rofs + ((CH * GL + 1) & ~1));  // [CH][Ny], 16-B aligned
     float* Bbuf = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(cent) +
                                            (((size_t)CH * n2 * 8 + 15) & ~(size_t)15));
     const Layout L = make_layout(kp);
     const float cap = kp.p.cap;
     const int64_t P = L.P;
-    const int64_t pl = item / kp.tiles_x;
-    const int32_t xt = (int32_t)(item - pl * kp.tiles_x);
-    const int32_t x0 = xt * TX;
-    const int32_t nr = min(TX, n1 - x0);
     int32_t pq6[4];
     {
         int64_t pp = pl;
@@ -398,6 +397,8 @@ __device__ __forceinline__ void stencil_r_item(
     const bool cel = g < GL;
     const int wid = tid >> 5, nw = T >> 5;
     const uint32_t lane = (uint32_t)tid & 31u;
+    const bool jlast = j == n2 - 1;
+    const int32_t wofs = 4 * g * SB + j;  // this thread's first window cell
 
     // the group order; admissible controls first, nadm of them
     if (tid == 0) s_nadm = nctl;
@@ -408,258 +409,269 @@ __device__ __forceinline__ void stencil_r_item(
             s_nadm = i;
     __syncthreads();
     const int nadm = s_nadm;
+    // one chunk holds every admissible control: its parameters, column
+    // entries and weights stay for all the plane's tiles
+    const bool keep = nadm <= CH;
 
-    const uint8_t* occ_h = occ + ((int64_t)pq6[0] * n1 + x0) * n2;
-    float best[4];
-    int bk[ARGMIN ? 4 : 1];
-    uint32_t live = 0;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        best[q] = cap;
-        if constexpr (ARGMIN) bk[q] = 0x7fffffff;
-        const int32_t a = 4 * g + q;
-        if (cel && a < nr && occ_h[a * n2 + j] == 0) live |= 1u << q;
-    }
-    const bool jlast = j == n2 - 1;
-    const int32_t wofs = 4 * g * SB + j;  // this thread's first window cell
-
-    uint64_t cv[2][16];  // the group's corner values, rows (4g, 4g+1) and (4g+2, 4g+3) paired
-    // corner values of the group that the control at position p starts: the
-    // planes of its record, rows from its x offset
-    auto load_group = [&](int p) {
-        const uint32_t* rec = prec + (size_t)(ord[p] & kCtlMask) * kURec;
-        const int32_t wbase = x0 + (int32_t)__ldg(rec + kUNT + 16) - 1;
-        const S* base[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int32_t r = min(max(wbase + 4 * g + k, 0), n1 - 1);
-            base[k] = Vin + (int64_t)r * n2 + j;
-        }
-#pragma unroll
-        for (int c = 0; c < 16; ++c) {
-            const int64_t off = (int64_t)__ldg(rec + kUNT + c) * P;
-            cv[0][c] = pk2(Conv<S>::ld(base[0] + off), Conv<S>::ld(base[1] + off));
-            cv[1][c] = pk2(Conv<S>::ld(base[2] + off), Conv<S>::ld(base[3] + off));
+    // a chunk's per-control parameters, a warp per control: its record's
+    // words 0-15 (w[16]) into words 16-31, words 16-19 (tau, tx, ty, -) and
+    // kUNT+16..19 (ox, oy, ok, nsub) into words 32-39, its first NI x
+    // increments from word 40 and its first NI y increments into the window
+    // buffers, as 16-byte asynchronous copies
+    auto stage_params = [&](int c0, int ch) {
+        const int32_t pieces = NI / 2, half = NI / 4;
+        for (int lp = wid; lp < ch; lp += nw) {
+            const uint32_t* rec = prec + (size_t)(ord[c0 + lp] & kCtlMask) * kURec;
+            for (int c = (int)lane; c < 6 + pieces; c += 32) {
+                if (c < 6) {
+                    cp_async16(wt + lp * RW + 16 + 4 * c, rec + (c < 5 ? 4 * c : kUNT + 16));
+                } else {
+                    const int32_t k = c - 6;
+                    if (k < half)
+                        cp_async16(wt + lp * RW + kRInc + 4 * k, rec + kUInc + 4 * k);
+                    else
+                        cp_async16(Bbuf + lp * NI + 4 * (k - half),
+                                   rec + kUInc + kStencilMaxSub + 4 * (k - half));
+                }
+            }
         }
     };
-    if (nadm > 0 && act) load_group(0);
+    // a chunk's column entries (a warp per control, a lane per column) --
+    // the lower column's byte offset and the y fraction
+    auto make_columns = [&](int ch) {
+        for (int lp = wid; lp < ch; lp += nw) {
+            for (int k = (int)lane; k < n2; k += 32) {
+                int32_t li;
+                float t;
+                succ_li_t(kp.g, Bbuf + lp * NI, kp.nsub, false, k, n1, n2, &li, &t);
+                cent[lp * n2 + k] = make_int2(min(max(li, 0), n2 - 1) * 4, __float_as_int(t));
+            }
+        }
+    };
+    // a chunk's duplicated weight pairs and next-group flags (a thread per
+    // control)
+    auto spread_weights = [&](int c0, int ch) {
+        for (int lp = tid; lp < ch; lp += T) {
+            float* a = wt + lp * RW;
+            float w[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) w[c] = a[16 + c];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) { a[2 * c] = w[c]; a[2 * c + 1] = w[c]; }
+            const int p1 = c0 + lp + 1;
+            a[kRNext] = __int_as_float((p1 < nadm && (ord[p1] & kGroupFirst)) ? 1 : 0);
+        }
+    };
 
+    uint64_t cv[2][16];  // the group's corner values, rows (4g, 4g+1) and (4g+2, 4g+3) paired
     int buf = 0;
-    for (int c0 = 0; c0 < nadm; c0 += CH) {
-        const int ch = min(CH, nadm - c0);
-        // stage the chunk's per-control data, a warp per control: its
-        // record's words 0-19 (w[16], tau, tx, ty, -) and kUNT+16..19 (ox,
-        // oy, ok, nsub) as six 16-byte pieces, its first NI x and y
-        // increments, and its mask words
-        {
-            const int32_t pieces = NI / 2, half = NI / 4;
-            const int32_t npc = 6 + pieces + TS / 4;
+    for (int32_t xt = t0; xt < t1; ++xt) {
+        const int32_t x0 = xt * TX;
+        const int32_t nr = min(TX, n1 - x0);
+        const uint8_t* occ_h = occ + ((int64_t)pq6[0] * n1 + x0) * n2;
+        const uint32_t* tmt = tmask + (size_t)(pl * kp.tiles_x + xt) * nctl * TS;
+        float best[4];
+        int bk[ARGMIN ? 4 : 1];
+        uint32_t live = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            best[q] = cap;
+            if constexpr (ARGMIN) bk[q] = 0x7fffffff;
+            const int32_t a = 4 * g + q;
+            if (cel && a < nr && occ_h[a * n2 + j] == 0) live |= 1u << q;
+        }
+        // corner values of the group that the control at position p starts:
+        // the planes of its record, rows from its x offset
+        auto load_group = [&](int p) {
+            const uint32_t* rec = prec + (size_t)(ord[p] & kCtlMask) * kURec;
+            const int32_t wbase = x0 + (int32_t)__ldg(rec + kUNT + 16) - 1;
+            const S* base[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int32_t r = min(max(wbase + 4 * g + k, 0), n1 - 1);
+                base[k] = Vin + (int64_t)r * n2 + j;
+            }
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                const int64_t off = (int64_t)__ldg(rec + kUNT + c) * P;
+                cv[0][c] = pk2(Conv<S>::ld(base[0] + off), Conv<S>::ld(base[1] + off));
+                cv[1][c] = pk2(Conv<S>::ld(base[2] + off), Conv<S>::ld(base[3] + off));
+            }
+        };
+        if (nadm > 0 && act) load_group(0);
+
+        for (int c0 = 0; c0 < nadm; c0 += CH) {
+            const int ch = min(CH, nadm - c0);
+            const bool fresh = !keep || xt == t0;  // this chunk's parameters are not staged yet
+            if (fresh) stage_params(c0, ch);
+            // the tile's mask words of the chunk's controls, a warp per control
             for (int lp = wid; lp < ch; lp += nw) {
-                const int u = ord[c0 + lp] & kCtlMask;
-                const uint32_t* rec = prec + (size_t)u * kURec;
-                const uint32_t* tm = tmask + ((size_t)(pl * kp.tiles_x + xt) * nctl + u) * TS;
-                for (int c = (int)lane; c < npc; c += 32) {
-                    if (c < 6) {
-                        cp_async16(wt + lp * RW + 4 * c, rec + (c < 5 ? 4 * c : kUNT + 16));
-                    } else if (c < 6 + pieces) {
-                        const int32_t k = c - 6;
-                        cp_async16(wt + lp * RW + kRWt + 4 * k,
-                                   rec + (k < half ? kUInc + 4 * k : kUInc + kStencilMaxSub + 4 * (k - half)));
-                    } else {
-                        const int32_t k = c - 6 - pieces;
-                        cp_async16(msk + lp * TS + 4 * k, tm + 4 * k);
-                    }
-                }
+                const uint32_t* tm = tmt + (size_t)(ord[c0 + lp] & kCtlMask) * TS;
+                for (int c = (int)lane; c < TS / 4; c += 32) cp_async16(msk + lp * TS + 4 * c, tm + 4 * c);
             }
             cp_async_commit();
             cp_async_wait_all();
-        }
-        __syncthreads();
-
-        // every staged control's successor entries from its increments, a
-        // warp per control and a lane per tile row or column: per live row
-        // group the four rows' window offsets (the lower corner's row from the
-        // window base, in bytes) and x fractions, then per column the lower
-        // column's byte offset and the y fraction
-        for (int lp = wid; lp < ch; lp += nw) {
-            const float* a = wt + lp * RW;
-            const int32_t wbase = x0 + __float_as_int(a[20]) - 1;
-            int32_t* re = reinterpret_cast<int32_t*>(rent + lp * GL * 2);
-            for (int k = (int)lane; k < 4 * GL + n2; k += 32) {
-                const bool row = k < 4 * GL;
-                if (row && k >= nr) {  // a tile row past the plane: no cell reads it
-                    re[(k >> 2) * 8 + (k & 3)] = 0;
-                    re[(k >> 2) * 8 + 4 + (k & 3)] = 0;
-                    continue;
-                }
-                int32_t li;
-                float t;
-                succ_li_t(kp.g, a + kRWt + (row ? 0 : NI), kp.nsub, row, row ? x0 + k : k - 4 * GL,
-                          n1, n2, &li, &t);
-                if (row) {
-                    re[(k >> 2) * 8 + (k & 3)] = min(max(li - wbase, 0), nr + 1) * SB4;
-                    re[(k >> 2) * 8 + 4 + (k & 3)] = __float_as_int(t);
-                } else {
-                    cent[lp * n2 + k - 4 * GL] =
-                        make_int2(min(max(li, 0), n2 - 1) * 4, __float_as_int(t));
-                }
-            }
-        }
-        __syncthreads();
-        // the increments are spent: rewrite each control's parameter area as
-        // its weights duplicated into FP32 pairs for the packed blend, then the
-        // eight parameter words (each thread its own controls)
-        for (int lp = tid; lp < ch; lp += T) {
-            float* a = wt + lp * RW;
-            float w[16], par[8];
-#pragma unroll
-            for (int c = 0; c < 16; ++c) w[c] = a[c];
-#pragma unroll
-            for (int c = 0; c < 8; ++c) par[c] = a[16 + c];
-#pragma unroll
-            for (int c = 0; c < 16; ++c) { a[2 * c] = w[c]; a[2 * c + 1] = w[c]; }
-#pragma unroll
-            for (int c = 0; c < 8; ++c) a[kRTau + c] = par[c];
-            const int p1 = c0 + lp + 1;
-            a[kRNext] = __int_as_float((p1 < nadm && (ord[p1] & kGroupFirst)) ? 1 : 0);
-            // bit 0 of a row group's first offset: its four rows are live and
-            // their successor rows consecutive
-            int4* ro = rent + lp * GL * 2;
-            for (int k = 0; k < GL; ++k) {
-                const int4 o = ro[2 * k];
-                const bool cons = 4 * k + 3 < nr && o.y == o.x + SB4 && o.z == o.x + 2 * SB4 &&
-                                  o.w == o.x + 3 * SB4;
-                if (cons) ro[2 * k].x = o.x | 1;
-            }
-        }
-        __syncthreads();
-
-        // the controls two at a time (one barrier per pair) while the second
-        // stays in the first's corner group, else one: blend into the pair's
-        // two window buffers -- the two FMA chains of each control
-        // interleaved, four independent chains per thread --, one barrier,
-        // then shift both
-        int lp = 0;
-        while (lp < ch) {
-            const bool two = lp + 1 < ch && __float_as_int(wt[lp * RW + kRNext]) == 0;
-            const float* wa = wt + lp * RW;
-            const float* wb = wa + RW;
-            float* BA = Bbuf + (2 * buf) * bsz;
-            float* BB = BA + bsz;
-            buf ^= 1;
-            if (act) {
-                if (two) {
-                    uint64_t a2[2] = {0ull, 0ull}, b2[2] = {0ull, 0ull};
-#pragma unroll
-                    for (int c4 = 0; c4 < 4; ++c4) {
-                        // (w, w) pairs of corners 4 c4 .. 4 c4 + 3
-                        const ulonglong2 pa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4];
-                        const ulonglong2 qa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4 + 1];
-                        const ulonglong2 pb = reinterpret_cast<const ulonglong2*>(wb)[2 * c4];
-                        const ulonglong2 qb = reinterpret_cast<const ulonglong2*>(wb)[2 * c4 + 1];
-#pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            a2[k] = fma2(pa.x, cv[k][4 * c4 + 0], a2[k]);
-                            b2[k] = fma2(pb.x, cv[k][4 * c4 + 0], b2[k]);
-                        }
-#pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            a2[k] = fma2(pa.y, cv[k][4 * c4 + 1], a2[k]);
-                            b2[k] = fma2(pb.y, cv[k][4 * c4 + 1], b2[k]);
-                        }
-#pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            a2[k] = fma2(qa.x, cv[k][4 * c4 + 2], a2[k]);
-                            b2[k] = fma2(qb.x, cv[k][4 * c4 + 2], b2[k]);
-                        }
-#pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            a2[k] = fma2(qa.y, cv[k][4 * c4 + 3], a2[k]);
-                            b2[k] = fma2(qb.y, cv[k][4 * c4 + 3], b2[k]);
-                        }
-                    }
-                    r_store_window(BA + wofs, a2, SB, jlast);
-                    r_store_window(BB + wofs, b2, SB, jlast);
-                } else {
-                    uint64_t a2[2] = {0ull, 0ull};
-#pragma unroll
-                    for (int c4 = 0; c4 < 4; ++c4) {
-                        const ulonglong2 pa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4];
-                        const ulonglong2 qa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4 + 1];
-#pragma unroll
-                        for (int k = 0; k < 2; ++k) {
-                            a2[k] = fma2(pa.x, cv[k][4 * c4 + 0], a2[k]);
-                            a2[k] = fma2(pa.y, cv[k][4 * c4 + 1], a2[k]);
-                            a2[k] = fma2(qa.x, cv[k][4 * c4 + 2], a2[k]);
-                            a2[k] = fma2(qa.y, cv[k][4 * c4 + 3], a2[k]);
-                        }
-                    }
-                    r_store_window(BA + wofs, a2, SB, jlast);
-                }
-                // the corner values are free now: if the control after this
-                // step starts a new group, its loads fly during the barrier
-                // and the shifts
-                const int last = two ? lp + 1 : lp;
-                if (__float_as_int(wt[last * RW + kRNext]) != 0) load_group(c0 + last + 1);
-            }
             __syncthreads();
-            if (cel) {
-                r_shift<ARGMIN>(wa, BA, rent + lp * GL * 2 + 2 * g,
-                                cent[lp * n2 + j], msk + lp * TS + 4 * wid, SB4, lane, cap,
-                                ARGMIN ? (int)(ord[c0 + lp] & kCtlMask) : 0, best, bk);
-                if (two)
-                    r_shift<ARGMIN>(wb, BB, rent + (lp + 1) * GL * 2 + 2 * g,
-                                    cent[(lp + 1) * n2 + j], msk + (lp + 1) * TS + 4 * wid, SB4,
-                                    lane, cap, ARGMIN ? (int)(ord[c0 + lp + 1] & kCtlMask) : 0,
-                                    best, bk);
-            }
-            lp += two ? 2 : 1;
-        }
-        __syncthreads();  // the chunk's shared data is read; the next chunk may stage
-    }
-    if constexpr (ARGMIN) {
-        // controls no cell of the plane admits: ties at the cap go to the
-        // lower table index
-        for (int p = nadm; p < nctl; ++p) {
-            const int u = ord[p] & kCtlMask;
+            if (fresh) make_columns(ch);
+            // the tile's row entries, a thread per (control, live row group):
+            // the four rows' window offsets (the lower corner's row from the
+            // window base, in bytes; bit 0 of the first set when the four rows
+            // are in the tile and their successor rows consecutive) and x
+            // fractions
+            for (int i = tid; i < ch * GL; i += T) {
+                const int lp = i / GL, k = i - lp * GL;
+                const float* a = wt + lp * RW;
+                const int32_t wbase = x0 + __float_as_int(a[kROx]) - 1;
+                int32_t off[4];
+                float t[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (best[q] == cap && u < bk[q]) bk[q] = u;
+                for (int q = 0; q < 4; ++q) {
+                    const int32_t row = 4 * k + q;
+                    off[q] = 0;
+                    t[q] = 0.0f;
+                    if (row < nr) {
+                        int32_t li;
+                        succ_li_t(kp.g, a + kRInc, kp.nsub, true, x0 + row, n1, n2, &li, &t[q]);
+                        off[q] = min(max(li - wbase, 0), nr + 1) * SB4;
+                    }
+                }
+                const bool cons = 4 * k + 3 < nr && off[1] == off[0] + SB4 &&
+                                  off[2] == off[0] + 2 * SB4 && off[3] == off[0] + 3 * SB4;
+                rofs[i] = make_uint2((uint32_t)(off[0] | (cons ? 1 : 0)) | ((uint32_t)off[1] << 16),
+                                     (uint32_t)off[2] | ((uint32_t)off[3] << 16));
+                rtx[i] = make_float4(t[0], t[1], t[2], t[3]);
+            }
+            // (the weight pairs and flags occupy words 0-31 and 35, which the
+            // two passes above do not read)
+            if (fresh) spread_weights(c0, ch);
+            __syncthreads();
+            // the controls two at a time (one barrier per pair) while the second
+            // stays in the first's corner group, else one: blend into the pair's
+            // two window buffers -- the two FMA chains of each control
+            // interleaved, four independent chains per thread --, one barrier,
+            // then shift both
+            int lp = 0;
+            while (lp < ch) {
+                const bool two = lp + 1 < ch && __float_as_int(wt[lp * RW + kRNext]) == 0;
+                const float* wa = wt + lp * RW;
+                const float* wb = wa + RW;
+                float* BA = Bbuf + (2 * buf) * bsz;
+                float* BB = BA + bsz;
+                buf ^= 1;
+                if (act) {
+                    if (two) {
+                        uint64_t a2[2] = {0ull, 0ull}, b2[2] = {0ull, 0ull};
+    #pragma unroll
+                        for (int c4 = 0; c4 < 4; ++c4) {
+                            // (w, w) pairs of corners 4 c4 .. 4 c4 + 3
+                            const ulonglong2 pa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4];
+                            const ulonglong2 qa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4 + 1];
+                            const ulonglong2 pb = reinterpret_cast<const ulonglong2*>(wb)[2 * c4];
+                            const ulonglong2 qb = reinterpret_cast<const ulonglong2*>(wb)[2 * c4 + 1];
+    #pragma unroll
+                            for (int k = 0; k < 2; ++k) {
+                                a2[k] = fma2(pa.x, cv[k][4 * c4 + 0], a2[k]);
+                                b2[k] = fma2(pb.x, cv[k][4 * c4 + 0], b2[k]);
+                            }
+    #pragma unroll
+                            for (int k = 0; k < 2; ++k) {
+                                a2[k] = fma2(pa.y, cv[k][4 * c4 + 1], a2[k]);
+                                b2[k] = fma2(pb.y, cv[k][4 * c4 + 1], b2[k]);
+                            }
+    #pragma unroll
+                            for (int k = 0; k < 2; ++k) {
+                                a2[k] = fma2(qa.x, cv[k][4 * c4 + 2], a2[k]);
+                                b2[k] = fma2(qb.x, cv[k][4 * c4 + 2], b2[k]);
+                            }
+    #pragma unroll
+                            for (int k = 0; k < 2; ++k) {
+                                a2[k] = fma2(qa.y, cv[k][4 * c4 + 3], a2[k]);
+                                b2[k] = fma2(qb.y, cv[k][4 * c4 + 3], b2[k]);
+                            }
+                        }
+                        r_store_window(BA + wofs, a2, SB, jlast);
+                        r_store_window(BB + wofs, b2, SB, jlast);
+                    } else {
+                        uint64_t a2[2] = {0ull, 0ull};
+    #pragma unroll
+                        for (int c4 = 0; c4 < 4; ++c4) {
+                            const ulonglong2 pa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4];
+                            const ulonglong2 qa = reinterpret_cast<const ulonglong2*>(wa)[2 * c4 + 1];
+    #pragma unroll
+                            for (int k = 0; k < 2; ++k) {
+                                a2[k] = fma2(pa.x, cv[k][4 * c4 + 0], a2[k]);
+                                a2[k] = fma2(pa.y, cv[k][4 * c4 + 1], a2[k]);
+                                a2[k] = fma2(qa.x, cv[k][4 * c4 + 2], a2[k]);
+                                a2[k] = fma2(qa.y, cv[k][4 * c4 + 3], a2[k]);
+                            }
+                        }
+                        r_store_window(BA + wofs, a2, SB, jlast);
+                    }
+                    // the corner values are free now: if the control after this
+                    // step starts a new group, its loads fly during the barrier
+                    // and the shifts
+                    const int last = two ? lp + 1 : lp;
+                    if (__float_as_int(wt[last * RW + kRNext]) != 0) load_group(c0 + last + 1);
+                }
+                __syncthreads();
+                if (cel) {
+                    r_shift<ARGMIN>(wa, BA, rtx + lp * GL + g, rofs + lp * GL + g,
+                                    cent[lp * n2 + j], msk + lp * TS + 4 * wid, SB4, lane, cap,
+                                    ARGMIN ? (int)(ord[c0 + lp] & kCtlMask) : 0, best, bk);
+                    if (two)
+                        r_shift<ARGMIN>(wb, BB, rtx + (lp + 1) * GL + g, rofs + (lp + 1) * GL + g,
+                                        cent[(lp + 1) * n2 + j], msk + (lp + 1) * TS + 4 * wid, SB4,
+                                        lane, cap, ARGMIN ? (int)(ord[c0 + lp + 1] & kCtlMask) : 0,
+                                        best, bk);
+                }
+                lp += two ? 2 : 1;
+            }
+            __syncthreads();  // the chunk's shared data is read; the next chunk may stage
         }
-    }
+        if constexpr (ARGMIN) {
+            // controls no cell of the plane admits: ties at the cap go to the
+            // lower table index
+            for (int p = nadm; p < nctl; ++p) {
+                const int u = ord[p] & kCtlMask;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (best[q] == cap && u < bk[q]) bk[q] = u;
+            }
+        }
 
-    // write V' and the residual partials
-    const S* Vp0 = Vin + pl * P + (int64_t)x0 * n2;
-    S* Vo0 = Vout + pl * P + (int64_t)x0 * n2;
-    double dsum = 0.0, dmax = 0.0;
-    if (cel) {
+        // write the tile's V' and its residual partials
+        const S* Vp0 = Vin + pl * P + (int64_t)x0 * n2;
+        S* Vo0 = Vout + pl * P + (int64_t)x0 * n2;
+        double dsum = 0.0, dmax = 0.0;
+        if (cel) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int32_t a = 4 * g + q;
-            if (a >= nr) break;
-            const int32_t e = a * n2 + j;
-            const S ov = Vp0[e];
-            const float old = (float)Conv<S>::val(ov);
-            const bool lv = (live >> q) & 1u;
-            if constexpr (ARGMIN)
-                argmin[L.rowmajor(x0 + a, j, pq6[0], pq6[1], pq6[2], pq6[3])] =
-                    lv ? (int16_t)bk[q] : (int16_t)-1;
-            if (lv && (best[q] < old || (kp.relax && old > 0.0f && best[q] != old))) {
-                const S nv = Conv<S>::template st<float>(best[q]);
-                const float nvT = (float)Conv<S>::val(nv);
-                Vo0[e] = nv;
-                const double d = fabs((double)old - (double)nvT);
-                dsum += d;
-                dmax = fmax(dmax, d);
-            } else {
-                Vo0[e] = ov;
+            for (int q = 0; q < 4; ++q) {
+                const int32_t a = 4 * g + q;
+                if (a >= nr) break;
+                const int32_t e = a * n2 + j;
+                const S ov = Vp0[e];
+                const float old = (float)Conv<S>::val(ov);
+                const bool lv = (live >> q) & 1u;
+                if constexpr (ARGMIN)
+                    argmin[L.rowmajor(x0 + a, j, pq6[0], pq6[1], pq6[2], pq6[3])] =
+                        lv ? (int16_t)bk[q] : (int16_t)-1;
+                if (lv && (best[q] < old || (kp.relax && old > 0.0f && best[q] != old))) {
+                    const S nv = Conv<S>::template st<float>(best[q]);
+                    const float nvT = (float)Conv<S>::val(nv);
+                    Vo0[e] = nv;
+                    const double d = fabs((double)old - (double)nvT);
+                    dsum += d;
+                    dmax = fmax(dmax, d);
+                } else {
+                    Vo0[e] = ov;
+                }
             }
         }
+        block_partial_at(dsum, dmax, part_sum, part_max, slot0 + (xt - t0));
     }
-    block_partial_at(dsum, dmax, part_sum, part_max, slot);
 }
 
-// The single-table sweep: one block per work item.
+// The single-table sweep: block = plane, all its tiles.
 template <typename S, bool ARGMIN, int KR>
 __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlocks)
     k_stencil_r(const S* __restrict__ Vin, S* __restrict__ Vout, const uint8_t* __restrict__ occ,
@@ -667,8 +679,9 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
                 const uint16_t* __restrict__ gord, double* part_sum, double* part_max,
                 int16_t* argmin) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    stencil_r_item<S, ARGMIN, KR>(Vin, Vout, occ, recs, tmask, kp, gord, part_sum, part_max,
-                                  argmin, blockIdx.x, blockIdx.x, smem_raw);
+    stencil_r_plane<S, ARGMIN, KR>(Vin, Vout, occ, recs, tmask, kp, gord, part_sum, part_max,
+                                   argmin, blockIdx.x, 0, kp.tiles_x,
+                                   (int64_t)blockIdx.x * kp.tiles_x, smem_raw);
 }
 
 // Many tables in one launch, as k_stencil_b_batch (pg_stencil_b.cuh) but
@@ -706,7 +719,10 @@ __global__ void __launch_bounds__(RShape<KR>::kMaxThreads, RShape<KR>::kMinBlock
         }
         const S* vin = static_cast<const S*>(tb.V[parity]);
         S* vout = const_cast<S*>(static_cast<const S*>(tb.V[1 - parity]));
-        stencil_r_item<S, false, KR>(vin, vout, tb.occ, tb.recs, tb.tmask, tb.kp, tb.gord,
-                                     part_sum, part_max, nullptr, it - tb.item0, it, smem_raw);
+        const int64_t item = it - tb.item0;  // (plane, tile)
+        const int64_t pl = item / tb.kp.tiles_x;
+        const int32_t xt = (int32_t)(item - pl * tb.kp.tiles_x);
+        stencil_r_plane<S, false, KR>(vin, vout, tb.occ, tb.recs, tb.tmask, tb.kp, tb.gord,
+                                      part_sum, part_max, nullptr, pl, xt, xt + 1, it, smem_raw);
     }
 }

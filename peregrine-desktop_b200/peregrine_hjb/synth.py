@@ -39,6 +39,9 @@ WORKLOADS = {
     # the large workload's planes and controls with 2 headings: the same
     # per-block work, a few GB on the device, for profiler captures
     "large_h2": dict(n=[96, 96, 2, 21, 21, 21], control_set="cube5", dt=0.03, rects=8),
+    # the out-of-core variant: 5.5e10 cells, 110 GB per table in FP16, swept a
+    # tile of x rows at a time from host memory
+    "xlarge_ooc": dict(n=[192, 192, 96, 25, 25, 25], control_set="cube5", dt=0.03, rects=8),
 }
 
 

@@ -66,3 +66,15 @@ def test_committed_profile_is_of_the_current_kernel(bench):
     traffic = bench.profiled_traffic()
     assert wipu is not None and 1.0 < wipu < 10.0
     assert traffic is not None and traffic > 2 * 4 * 5_462_360_064  # at least V in and out
+
+
+def test_converge_error_helper_over_reached_cells(bench):
+    """max / RMS |V - ref| over the reached cells (0 < ref < cap - 1 ms),
+    chunked: unreached cells (ref 0 or at the cap) do not count."""
+    import numpy as np
+    ref = np.array([0.0, 1.0, 2.0, 30.0, 29.9995, 3.0], np.float32)
+    V = np.array([5.0, 1.5, 2.0, 10.0, 1.0, 2.75], np.float32)
+    mx, rms, n = bench._max_rms_over(V, ref, 30.0, "cpu", chunk=4)
+    assert n == 3
+    assert mx == 0.5
+    assert abs(rms - np.sqrt((0.25 + 0.0 + 0.0625) / 3)) < 1e-12
