@@ -595,6 +595,7 @@ def run_converge(args, local_rank):
             "error_over": "reached cells (0 < V < cap - 1 ms)", "fp32": rows,
             "maxnorm_every_25_sweeps": trace,
             "time_to_converge_s": {"fp32": min(ok) if ok else None}}
+    print(json.dumps(line), flush=True)  # the FP32 record, before the longer FP16 leg
     if "fp16" in args.storages.split(",") and rows:
         # one FP16 + FP32-polish solve, at the loosest tolerance whose FP32
         # table met 2 ms (the polish has to reach the same point)
@@ -608,7 +609,7 @@ def run_converge(args, local_rank):
                          "polish_sweeps": res.polish_iterations,
                          "kernel_s": res.kernel_ms / 1000.0, "max_err": mx, "rms_err": rms}]
         line["time_to_converge_s"]["fp16"] = res.kernel_ms / 1000.0 if mx <= 2e-3 else None
-    print(json.dumps(line), flush=True)
+        print(json.dumps(line), flush=True)
     return 0
 
 
