@@ -108,5 +108,6 @@ def test_register_sweep_at_the_fixed_point(pr, gold):
     frac = Vo / sc - np.floor(Vo / sc)
     far = (np.abs(frac - 0.5) * sc > FAST_MAX) & (Vo < cap)
     w16, g16 = want.view(np.uint16), card.view(np.uint16)
-    assert far.mean() > 0.5
+    # |frac - 0.5| > 0.2 holds for ~60 % of the reached cells
+    assert far.sum() > 0.5 * np.count_nonzero(Vo < cap)
     assert np.array_equal(w16[far], g16[far])
