@@ -284,11 +284,12 @@ __device__ __forceinline__ void r_store_window(float* bw, const uint64_t* a2, in
 // group (dead rows read row 0 and have no mask bit), kept where the control
 // is admissible.  wu: the control's parameter area; B: its window; rt, rp:
 // its row group's x fractions and packed window offsets; cc: its column
-// entry; mk: the warp's four mask words; u: its table index (argmin only).
+// entry; mk: the warp's four mask words; lbit: the thread's bit in them
+// (1 << lane); u: its table index (argmin only).
 template <bool ARGMIN>
 __device__ __forceinline__ void r_shift(const float* wu, const float* B, const float4* rt,
                                         const uint2* rp, const int2 cc, const uint32_t* mk,
-                                        int32_t SB4, uint32_t lane, float cap, int u, float* best,
+                                        int32_t SB4, uint32_t lbit, float cap, int u, float* best,
                                         int* bk) {
     const float tau = wu[kRTau];
     const uint2 ro = *rp;
@@ -322,7 +323,7 @@ __device__ __forceinline__ void r_shift(const float* wu, const float* B, const f
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const bool adm = (mw[q] >> lane) & 1u;
+        const bool adm = (mw[q] & lbit) != 0u;
         if constexpr (ARGMIN) {
             const float cvl = adm ? fminf(tau + fminf(val[q], cap), cap) : cap;
             // equal values go to the lower table index, which is what the
@@ -397,6 +398,7 @@ __device__ __forceinline__ void stencil_r_plane(
     const bool cel = g < GL;
     const int wid = tid >> 5, nw = T >> 5;
     const uint32_t lane = (uint32_t)tid & 31u;
+    const uint32_t lbit = 1u << lane;  // the thread's bit in its warp's mask words
     const bool jlast = j == n2 - 1;
     const int32_t wofs = 4 * g * SB + j;  // this thread's first window cell
 
@@ -616,12 +618,12 @@ __device__ __forceinline__ void stencil_r_plane(
                 __syncthreads();
                 if (cel) {
                     r_shift<ARGMIN>(wa, BA, rtx + lp * GL + g, rofs + lp * GL + g,
-                                    cent[lp * n2 + j], msk + lp * TS + 4 * wid, SB4, lane, cap,
+                                    cent[lp * n2 + j], msk + lp * TS + 4 * wid, SB4, lbit, cap,
                                     ARGMIN ? (int)(ord[c0 + lp] & kCtlMask) : 0, best, bk);
                     if (two)
                         r_shift<ARGMIN>(wb, BB, rtx + (lp + 1) * GL + g, rofs + (lp + 1) * GL + g,
                                         cent[(lp + 1) * n2 + j], msk + (lp + 1) * TS + 4 * wid, SB4,
-                                        lane, cap, ARGMIN ? (int)(ord[c0 + lp + 1] & kCtlMask) : 0,
+                                        lbit, cap, ARGMIN ? (int)(ord[c0 + lp + 1] & kCtlMask) : 0,
                                         best, bk);
                 }
                 lp += two ? 2 : 1;
