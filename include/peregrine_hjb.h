@@ -249,12 +249,13 @@ int pg_set_wait_timeout(pg_ctx* ctx, double seconds);
 /* Number of this library's kernel launches since the context was created. */
 int pg_launch_count(pg_ctx* ctx, int64_t* launches);
 
-/* Rows of one plane per block of the blend-then-shift sweeps (the tile
+/* Rows of one plane per tile of the blend-then-shift sweeps (the tile
  * shape the autotuner picks): 1 <= rows <= Nx, and rows * Ny <= 1024 (the
- * re-reading blend) or (rows + 3) * Ny <= 2048 (the register-resident blend,
- * whose window has 3 more rows); a kernel whose limit the rows exceed is not
- * used.  No counterpart in the reference (its kernel has one thread per
- * cell). */
+ * re-reading blend) or ceil((rows + 3) / 4) * Ny <= 512 (the register-
+ * resident blend: its window has 3 more rows than the tile, and a thread
+ * owns four window rows of one column); a kernel whose limit the rows
+ * exceed is not used.  No counterpart in the reference (its kernel has one
+ * thread per cell). */
 int pg_set_tile_rows(pg_ctx* ctx, int32_t rows);
 
 /* ------------------------------------------------------------------ */

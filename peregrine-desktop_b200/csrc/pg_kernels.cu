@@ -837,10 +837,7 @@ cudaError_t launch_stencil_prep(const uint8_t* occ, const KParams& kp, const flo
                                 cudaStream_t st, int64_t* launches) {
     size_t smem = stencil_prep_smem(kp.nctl, kp.nsub);
     const size_t tab = stencil_prep_tab_smem(kp.nctl, kp.g.n[1]);
-    // the column-table path indexes a plane's (control, row, word) items in
-    // 32 bits
-    const int coltab = kp.g.n[1] <= 255 && kp.nchk <= 4 && smem + tab <= 200 * 1024 &&
-                       (int64_t)kp.nctl * kp.g.n[0] * mask_words(kp.g.n[1]) < 0x7fffffffLL;
+    const int coltab = kp.g.n[1] <= 255 && kp.nchk <= 4 && smem + tab <= 200 * 1024;
     if (coltab) smem += tab;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static std::atomic<uint64_t> attr_set{0};

@@ -155,12 +155,9 @@ __global__ void __launch_bounds__(256)
             tab[it] = word;
         }
         __syncthreads();
-        // a plane's items fit 32 bits (nctl * n1 * W < 2^31, checked by the
-        // launcher), so the index arithmetic stays in 32 bits
-        const int32_t per_u = n1 * W;
-        for (int32_t it = threadIdx.x; it < (int32_t)items; it += blockDim.x) {
-            const int u = it / per_u;
-            const int32_t rem = it - u * per_u;
+        for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
+            const int u = (int)(it / ((int64_t)n1 * W));
+            const int32_t rem = (int32_t)(it - (int64_t)u * n1 * W);
             const int32_t i1 = rem / W, w = rem - i1 * W;
             uint32_t bits = 0;
             if (sok[u]) {
