@@ -45,10 +45,16 @@ def profile_path():
     return os.path.join(ROOT, "profiles", f"k_stencil_r_{WORKLOAD}_fp32.md")
 
 
-def kernel_source_sha():
+def kernel_source_sha(path=None):
+    """SHA-256 of the sweep kernel's code: pg_stencil_r.cuh with its //
+    comments, trailing blanks and blank lines removed, so that editing a
+    comment does not retire a profile of the same code."""
     import hashlib
-    with open(KERNEL_SOURCE, "rb") as fh:
-        return hashlib.sha256(fh.read()).hexdigest()
+    import re
+    with open(path or KERNEL_SOURCE, encoding="utf-8") as fh:
+        lines = [re.sub(r"//.*$", "", ln).rstrip() for ln in fh.read().splitlines()]
+    code = "\n".join(ln for ln in lines if ln)
+    return hashlib.sha256(code.encode("utf-8")).hexdigest()
 
 
 def peaks():

@@ -17,24 +17,26 @@
 //   k_stencil_tmask (once per tiling) regroups the admissibility mask per
 //   (plane, tile, control) in the order the sweep's threads read it;
 //
-//   k_stencil_r: block = (plane, tile of TX rows).  Thread (g, j) of the
-//   first G * Ny owns column j of the four window rows 4g .. 4g+3 and of the
-//   tile cells in those rows.  The block stages its controls' weights, tau,
-//   offsets, substep increments and mask words into shared memory with
-//   asynchronous copies (a chunk of controls at a time when they do not all
-//   fit), computes from the increments every control's per-row and
-//   per-column successor corners and fractions, and walks the controls in
+//   k_stencil_r: block = plane, its tiles of TX rows one after another.
+//   Thread (g, j) of the first G * Ny owns column j of the four window rows
+//   4g .. 4g+3 and of the tile cells in those rows.  Once per plane the
+//   block stages its controls' weights, tau, offsets and substep increments
+//   into shared memory with asynchronous copies and computes every
+//   control's per-column successor corners and fractions; per tile it
+//   stages the controls' mask words and computes their per-row successor
+//   corners and fractions (all of it per tile, a chunk of controls at a
+//   time, when the controls do not all fit).  It walks the controls in
 //   group order, two per step while both are in one group.  At the first
 //   control of a group each thread loads the 16 corner values of its four
 //   window cells into registers; for every control it blends them with the
 //   control's 16 weights (16 FMAs per window cell, two cells per packed
 //   fma.rn.f32x2, the two controls' chains interleaved, nothing re-read)
 //   into the shared window; one barrier per step; then it shifts: its four
-//   cells lie in consecutive rows of one
-//   column, and the successor rows of consecutive rows are nearly always
-//   consecutive too, so the four bilinear steps read five window rows (ten
-//   values) instead of eight, the column entry once, the row entries and
-//   the mask words as one vector each.
+//   cells lie in consecutive rows of one column, and the successor rows of
+//   consecutive rows are nearly always consecutive too, so the four
+//   bilinear steps read five window rows (ten values) instead of eight, the
+//   column entry once, the row entries and the mask words as one vector
+//   each.
 //
 // The arithmetic is k_stencil_b's, operation for operation: the same FMA
 // chain over the corners in record order, the same per-row / per-column

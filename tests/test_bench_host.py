@@ -78,3 +78,17 @@ def test_converge_error_helper_over_reached_cells(bench):
     assert n == 3
     assert mx == 0.5
     assert abs(rms - np.sqrt((0.25 + 0.0 + 0.0625) / 3)) < 1e-12
+
+
+def test_code_hash_ignores_comments_not_code(bench, tmp_path):
+    """A profile stays the current kernel's through comment edits, and only
+    through them: the hash is of the code without // comments and blank
+    lines."""
+    a = tmp_path / "a.cuh"
+    a.write_text("// header\nint f(int x) {  // note\n    return x + 1;\n}\n")
+    b = tmp_path / "b.cuh"
+    b.write_text("// another header\n\nint f(int x) {\n    return x + 1;  // other note\n}\n")
+    c = tmp_path / "c.cuh"
+    c.write_text("int f(int x) {\n    return x + 2;\n}\n")
+    assert bench.kernel_source_sha(str(a)) == bench.kernel_source_sha(str(b))
+    assert bench.kernel_source_sha(str(a)) != bench.kernel_source_sha(str(c))
