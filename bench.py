@@ -651,6 +651,40 @@ def run_ooc(args, local_rank):
     return 0
 
 
+def run_batch(args, local_rank):
+    """Batched sweeps against sequential ones: --tables tables drawn from the
+    batch workload's distribution (positions 24-48, headings 16-32, velocity
+    axes 9-15, 125 controls, each its own drivetrain, target and obstacles),
+    FP32.  Sequential: each table alone in its own context, --steps sweeps
+    timed on the device after 2 warm-up sweeps, summed over the tables.
+    Batched: all tables in one batch, --steps sweeps per table in persistent
+    launches captured as a CUDA graph, device time per sweep of all tables."""
+    from peregrine_hjb import _lib
+    from peregrine_hjb import batch as pb
+    probs = pb.batch_problems(args.tables, seed=0)
+    seq_ms, cells = 0.0, 0
+    for pr in probs:
+        with _lib.Context(local_rank) as ctx:
+            ctx.load_problem(pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.ctl, "fp32")
+            ctx.solve(pr.seeds, 0, 0.0, _lib.default_opts(kernel=_lib.KERNEL_STENCIL))
+            seq_ms += ctx.time_sweeps(2, args.steps, _lib.KERNEL_STENCIL)
+        cells += pr.ncells
+    with _lib.Batch(local_rank, "fp32") as b:
+        for pr in probs:
+            b.add(pr.grid.to_c(), pr.model.to_c(), pr.params, pr.occ, pr.seeds, pr.ctl)
+        b.solve(2, 0.0, 0, True)
+        res = b.solve(args.steps, 0.0, 0, True)
+    batch_ms = res.kernel_ms / max(res.sweeps, 1)
+    line = {"report": "batched_sweeps", "tables": len(probs), "cells": cells,
+            "controls": int(probs[0].nctl), "storage": "fp32", "sweeps_timed": int(res.sweeps),
+            "sequential_ms_per_sweep_of_all_tables": seq_ms,
+            "batched_ms_per_sweep_of_all_tables": batch_ms,
+            "batched_vs_sequential": seq_ms / batch_ms if batch_ms > 0 else None,
+            "graph": bool(res.graph)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -673,6 +707,10 @@ def main():
                     help="out-of-core rounds of the workload (e.g. --workload xlarge_ooc "
                          "--storage fp16) instead of the throughput line")
     ap.add_argument("--rounds", type=int, default=1, help="rounds of --ooc")
+    ap.add_argument("--batch", action="store_true",
+                    help="batched against sequential sweeps of --tables tables of the batch "
+                         "workload's distribution")
+    ap.add_argument("--tables", type=int, default=16, help="tables of --batch")
     ap.add_argument("--storages", default="fp32,fp16,bf16,q16,q16-nopolish",
                     help="storages of the accuracy report; -nopolish: no FP32 polish")
     ap.add_argument("--no-fp64", action="store_true",
@@ -695,6 +733,8 @@ def main():
         return run_converge(args, local_rank)
     if args.ooc:
         return run_ooc(args, local_rank)
+    if args.batch:
+        return run_batch(args, local_rank)
     if world > 1:
         import datetime
         import torch
